@@ -1,0 +1,225 @@
+/*
+ * xcal.h -- C ABI of libxcal.so, the sm_100a implementation of the per-iteration
+ * hot path of XCALibre's unstructured finite-volume pressure-velocity solver.
+ *
+ * The reference (module FVM_1D, Julia) has no FFI of its own; its operator-level
+ * seam is a set of Julia functions taking Julia structs with 1-based Int64/Float64
+ * vectors.  Every entry point below names the reference function it replaces
+ * (paths relative to the reference project root).  A Julia `ccall` shim binds
+ * these symbols one to one.
+ *
+ * Conventions
+ *   - All indices crossing this ABI are 1-based int64 (Julia's native layout);
+ *     the library converts them to 0-based int32 for the device.
+ *   - Host arrays are owned by the caller; the library copies what it needs into
+ *     its own device buffers and never keeps a host pointer after a call returns.
+ *   - Every function returns an int status: XCAL_OK (0) or a negative XCAL_ERR_*
+ *     code.  xcal_last_error() returns the message of the last failure on a
+ *     context.  A context is used by one host thread at a time; each context
+ *     owns one CUDA stream.
+ */
+#ifndef XCAL_H
+#define XCAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+  XCAL_OK = 0,
+  XCAL_ERR_ARG = -1,         /* invalid argument or size */
+  XCAL_ERR_MESH = -2,        /* inconsistent or corrupt mesh */
+  XCAL_ERR_OOM = -3,         /* device allocation failed */
+  XCAL_ERR_CUDA = -4,        /* CUDA runtime error */
+  XCAL_ERR_NAN = -5,         /* non-finite field values (only with XCAL_FLAG_ABORT_ON_NAN) */
+  XCAL_ERR_TIMEOUT = -6,     /* a bounded device-side wait expired */
+  XCAL_ERR_STATE = -7,       /* call out of order (e.g. run before case setup) */
+  XCAL_ERR_IO = -8,          /* file could not be read */
+  XCAL_ERR_UNSUPPORTED = -9  /* option not implemented */
+};
+
+/* ------------------------------------------------------------ enumerations */
+/* boundary condition types: src/Discretise/Discretise_0_types.jl:31-78 */
+enum { XCAL_BC_DIRICHLET = 0, XCAL_BC_NEUMANN = 1, XCAL_BC_KWALL = 2,
+       XCAL_BC_OMEGAWALL = 3, XCAL_BC_NUTWALL = 4 };
+/* schemes: src/Discretise/Discretise_0_types.jl:13-21 */
+enum { XCAL_TIME_STEADY = 0, XCAL_TIME_EULER = 1 };
+enum { XCAL_DIV_LINEAR = 0, XCAL_DIV_UPWIND = 1 };
+enum { XCAL_LAP_LINEAR = 0 };
+enum { XCAL_GRAD_ORTHOGONAL = 0, XCAL_GRAD_MIDPOINT = 1 };
+/* Krylov solvers (Krylov.jl 0.9.5 CgSolver / BicgstabSolver) */
+enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
+/* preconditioners: src/Solve/Preconditioners/preconditioners_0_types.jl:7-12 */
+enum { XCAL_PRECON_DILU = 0, XCAL_PRECON_JACOBI = 1, XCAL_PRECON_NORMDIAG = 2,
+       XCAL_PRECON_NONE = 3 };
+/* turbulence model: src/RANSModels/RANSModels_0_types.jl:10, RANSModels_kOmega.jl:127 */
+enum { XCAL_MODEL_LAMINAR = 0, XCAL_MODEL_KOMEGA = 1 };
+/* cell renumbering applied once at mesh upload */
+enum { XCAL_RENUMBER_NONE = 0,      /* keep the caller's numbering (exact reference order) */
+       XCAL_RENUMBER_RCM = 1,       /* reverse Cuthill-McKee */
+       XCAL_RENUMBER_COLOR = 2 };   /* multicolour classes (2 for quad/hex meshes) */
+/* arithmetic of the device path */
+enum { XCAL_PREC_FP64 = 0, XCAL_PREC_MIXED = 1 };
+/* fields addressable through xcal_field_set/get */
+enum { XCAL_FIELD_UX = 0, XCAL_FIELD_UY = 1, XCAL_FIELD_UZ = 2, XCAL_FIELD_P = 3,
+       XCAL_FIELD_K = 4, XCAL_FIELD_OMEGA = 5, XCAL_FIELD_NUT = 6 };
+/* context flags */
+enum { XCAL_FLAG_ABORT_ON_NAN = 1u, XCAL_FLAG_PHASE_TIMERS = 2u };
+
+/* ----------------------------------------------------------------- mesh */
+/*
+ * The reference's flattened mesh (Mesh.Mesh2 after update_mesh_format,
+ * src/Mesh/Mesh_0_types.jl:34-94, src/Mesh/Mesh2D/Mesh2D_0_update_mesh.jl:5-142).
+ * Faces 1..nbfaces are the boundary faces (the reference builder numbers them
+ * first, src/UNV2/UNV2_3_builder.jl:97-115).  Per-cell face lists contain the
+ * internal faces only, in the order of cell.faces_range.
+ */
+typedef struct {
+  int64_t ncells, nfaces, nbfaces;
+  int32_t dim;                      /* 2 = reference 2D path; 3 = hexahedral extension */
+  const double *cell_centre;        /* [ncells*3] */
+  const double *cell_volume;        /* [ncells]   */
+  const int64_t *cell_faces_ptr;    /* [ncells+1] 1-based start of faces_range; ptr[n]=total+1 */
+  const int64_t *cell_faces;        /* [total] 1-based face ids (mesh.cell_faces) */
+  const int64_t *cell_neighbours;   /* [total] 1-based (mesh.cell_neighbours) */
+  const int64_t *cell_nsign;        /* [total] +1/-1 (mesh.cell_nsign) */
+  const int64_t *face_owner;        /* [nfaces*2] 1-based ownerCells */
+  const double *face_centre;        /* [nfaces*3] */
+  const double *face_normal;        /* [nfaces*3] */
+  const double *face_e;             /* [nfaces*3] */
+  const double *face_area;          /* [nfaces] */
+  const double *face_delta;         /* [nfaces] */
+  const double *face_weight;        /* [nfaces] */
+  int64_t npatches;
+  const int64_t *patch_ptr;         /* [npatches+1] 0-based offsets into patch_faces/cells */
+  const int64_t *patch_faces;       /* 1-based boundary.facesID, concatenated */
+  const int64_t *patch_cells;       /* 1-based boundary.cellsID, concatenated */
+} xcal_mesh_desc;
+
+/* ------------------------------------------------------------ case config */
+/* One boundary condition: Dirichlet(:name, value) etc., patch given by its
+ * 0-based index in the mesh's patch list (boundary_index, src/Mesh/Mesh_1_functions.jl:20-30).
+ * Wall-function constants default to (0.41, 0.075, 0.09, 5.2, 9.8)
+ * (src/Discretise/Discretise_0_types.jl:60-78). */
+typedef struct {
+  int32_t patch;
+  int32_t type;
+  double value[3];
+  double kappa, beta1, cmu, B, E;
+} xcal_bc;
+
+typedef struct { int32_t time, divergence, laplacian, gradient; } xcal_schemes;   /* set_schemes */
+typedef struct { int32_t solver, preconditioner, itmax, pad;
+                 double convergence, relax, atol, rtol; } xcal_solver_cfg;       /* set_solver */
+
+typedef struct {
+  int32_t model;                    /* XCAL_MODEL_* */
+  int32_t precision;                /* XCAL_PREC_* */
+  double nu;                        /* ConstantScalar viscosity */
+  xcal_schemes schemes_U, schemes_p, schemes_k, schemes_omega;
+  xcal_solver_cfg solver_U, solver_p, solver_k, solver_omega;
+  int32_t iterations, write_interval;   /* set_runtime */
+  double dt;
+  int32_t has_pref, pad0;               /* simple!(...; pref) */
+  double pref;
+  int32_t nbc_U, nbc_p, nbc_k, nbc_omega, nbc_nut, pad1;
+  const xcal_bc *bc_U, *bc_p, *bc_k, *bc_omega, *bc_nut;  /* @assign! order */
+} xcal_case;
+
+/* ------------------------------------------------------------ entry points */
+typedef struct xcal_ctx_s *xcal_ctx;
+
+/* Context life cycle.  No reference counterpart (the reference is host-only). */
+int xcal_ctx_create(int device, uint32_t flags, xcal_ctx *out);
+int xcal_ctx_destroy(xcal_ctx ctx);
+int xcal_last_error(xcal_ctx ctx, char *buf, size_t n);
+int xcal_version(int *major, int *minor);
+
+/* Mesh construction on the host (replaces build_mesh + update_mesh_format,
+ * src/UNV2/UNV2_3_builder.jl:3-23 and src/Mesh/Mesh2D/Mesh2D_0_update_mesh.jl:5-142).
+ * Builds the reference-format mesh from a UNV file; the mesh is held inside a
+ * host-side handle whose arrays are read back with xcal_hmesh_counts/arrays. */
+typedef struct xcal_hmesh_s *xcal_hmesh;
+int xcal_hmesh_build_unv(const char *path, double scale, xcal_hmesh *out, char *err, size_t nerr);
+int xcal_hmesh_counts(xcal_hmesh m, int64_t counts[8]);  /* ncells,nfaces,nbfaces,total,npatches,patchlen,nnodes,names_len */
+int xcal_hmesh_desc(xcal_hmesh m, xcal_mesh_desc *desc);  /* pointers valid until free */
+int xcal_hmesh_patch_names(xcal_hmesh m, char *buf, size_t n);   /* '\n'-separated */
+int xcal_hmesh_free(xcal_hmesh m);
+/* Host-only helpers (no device needed): wrap a caller mesh, renumber it the way
+ * xcal_mesh_upload does (perm[i] = 1-based new index of cell i+1), and build
+ * the device CSR pattern and DILU level sets of a host mesh. */
+int xcal_hmesh_from_desc(const xcal_mesh_desc *desc, xcal_hmesh *out, char *err, size_t nerr);
+int xcal_hmesh_renumber(xcal_hmesh m, int32_t renumber, xcal_hmesh *out, int64_t *perm);
+int xcal_hmesh_csr(xcal_hmesh m, int64_t *nnz, int32_t *row_ptr, int32_t *col,
+                   int32_t *flevel, int32_t *blevel, int32_t *nlevels);
+
+/* Upload a mesh to the device (the reference keeps the mesh in host structs;
+ * this replaces Equation(mesh), src/ModelFramework/ModelFramework_0_types.jl:90-125,
+ * and the preconditioner set-up, src/Solve/Preconditioners/preconditioners_2_functions.jl:4-13). */
+int xcal_mesh_upload(xcal_ctx ctx, const xcal_mesh_desc *mesh, int32_t renumber);
+/* perm[i] = 1-based device index of the caller's cell i+1 */
+int xcal_mesh_permutation(xcal_ctx ctx, int64_t *perm, int64_t n);
+/* The mesh the device works on, in the reference layout (equal to the input for
+ * XCAL_RENUMBER_NONE).  Arrays must be sized with the input mesh's counts. */
+int xcal_mesh_export(xcal_ctx ctx, int64_t *cell_faces_ptr, int64_t *cell_faces,
+                     int64_t *cell_neighbours, int64_t *cell_nsign, int64_t *face_owner,
+                     double *cell_centre, double *cell_volume, double *face_centre,
+                     double *face_normal, double *face_e, double *face_area,
+                     double *face_delta, double *face_weight, int64_t *patch_faces,
+                     int64_t *patch_cells);
+/* Integer device structures: CSR pattern (0-based, rows in device numbering)
+ * and DILU forward/backward level of every row. */
+int xcal_mesh_csr(xcal_ctx ctx, int64_t *nnz, int32_t *row_ptr, int32_t *col,
+                  int32_t *flevel, int32_t *blevel, int32_t *nlevels);
+
+/* Model and configuration (RANS{...}, @assign!, set_schemes, set_solver,
+ * set_runtime, Configuration: src/RANSModels/RANSModels_0_types.jl:22-31,
+ * src/Discretise/Discretise_0_types.jl:80-181, src/Solve/Solve_1_api.jl:5-30,
+ * src/Simulate/Simulate_0_types.jl:3-8). */
+int xcal_case_setup(xcal_ctx ctx, const xcal_case *cfg);
+
+/* Field values in the caller's numbering (initialise!, src/Fields/Fields_0_types.jl:205-222). */
+int xcal_field_set(xcal_ctx ctx, int32_t field, const double *host, int64_t n);
+int xcal_field_get(xcal_ctx ctx, int32_t field, double *host, int64_t n);
+
+/* simple!(model, config; pref) -> (R_ux, R_uy, R_p): src/Solvers/Solvers_1_SIMPLE.jl:3-231.
+ * Runs `iterations` SIMPLE iterations (one persistent device kernel), writes the
+ * residual histories (entries after convergence stay 1.0 as in the reference),
+ * and optionally the Krylov iteration count of every solve (krylov_iters has
+ * 5*iterations entries: ux, uy, uz, p, spare; may be NULL).  *done receives the
+ * number of iterations executed (fewer when all residuals fall below 1e-7).
+ * R_uz may be NULL for 2D meshes. */
+int xcal_simple_run(xcal_ctx ctx, int32_t iterations, double *R_ux, double *R_uy,
+                    double *R_uz, double *R_p, int32_t *krylov_iters, int32_t *done);
+/* piso!(model, config; pref): src/Solvers/Solvers_2_PISO.jl:3-238 (2 correctors). */
+int xcal_piso_run(xcal_ctx ctx, int32_t iterations, double *R_ux, double *R_uy,
+                  double *R_uz, double *R_p, int32_t *krylov_iters, int32_t *done);
+/* Device time of the last run, and per-phase device cycle counters when the
+ * context was created with XCAL_FLAG_PHASE_TIMERS. */
+int xcal_last_run_stats(xcal_ctx ctx, double *ms, double *phase_cycles, int32_t nphases);
+
+/* Assembled linear systems of the last iteration, in device numbering, CSR order:
+ * which = 0 momentum (A shared by ux/uy/uz, b per component), 1 pressure.
+ * Mirrors ux_eqn.equation / p_eqn.equation (src/ModelFramework/ModelFramework_0_types.jl:83-89). */
+int xcal_equation_get(xcal_ctx ctx, int32_t which, double *vals, double *b0,
+                      double *b1, double *b2);
+
+/* Standalone linear solve on a caller CSR matrix: run!(eqn, setup) with
+ * Krylov.jl solve!(solver, A, b, x0; M=P, itmax, atol, rtol) and the DILU/Jacobi
+ * preconditioners (src/Solve/Solve_1_api.jl:32-46,
+ * src/Solve/Preconditioners/preconditioners_1_DILU.jl:5-168).
+ * row_ptr/col are 0-based; columns sorted within each row; pattern symmetric.
+ * x holds x0 on entry and the solution on exit. */
+int xcal_linear_solve(xcal_ctx ctx, int32_t solver, int32_t precon, int64_t n,
+                      const int32_t *row_ptr, const int32_t *col, const double *val,
+                      const double *b, double *x, int32_t itmax, double atol,
+                      double rtol, int32_t *niter, double *final_rnorm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XCAL_H */

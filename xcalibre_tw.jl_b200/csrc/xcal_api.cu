@@ -1,0 +1,702 @@
+// C ABI of libxcal.so (include/xcal.h): contexts, mesh upload, case set-up,
+// field transfer, runs of the persistent device program, standalone solves.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/xcal.h"
+#include "host_mesh.h"
+#include "xcal_kernel.h"
+
+using namespace xcal;
+
+namespace {
+
+// Device allocations of one context, released together.
+struct DevBuf {
+  std::vector<void *> ptrs;
+  ~DevBuf() { release(); }
+  void release() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+  template <class T>
+  T *alloc(size_t n) {
+    if (n == 0) n = 1;
+    void *p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return (T *)p;
+  }
+};
+
+}  // namespace
+
+struct xcal_ctx_s {
+  int device = 0;
+  uint32_t flags = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  bool have_mesh = false, have_case = false;
+  HostMesh user, mesh;
+  std::vector<int64_t> perm;   // user cell -> device cell
+  Prep prep;
+  int ns = 2;
+  int mode = SYNC_GRID, nblocks = 1;
+  DevBuf mbuf, cbuf, rbuf;     // mesh, case, run buffers
+  KParams hp;
+  KParams *dp = nullptr;
+  int run_cap = 0;
+  double last_ms = 0.0;
+  double *pin = nullptr;       // pinned staging [n*3]
+  size_t pin_n = 0;
+  std::vector<BcEntry> tabU, tabP;
+};
+
+struct xcal_hmesh_s {
+  HostMesh M;
+};
+
+static int fail(xcal_ctx c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+#define CUDA_TRY(c, x)                                                            \
+  do {                                                                            \
+    cudaError_t e_ = (x);                                                         \
+    if (e_ != cudaSuccess) return fail(c, XCAL_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+static int upload(xcal_ctx c, DevBuf &buf, T *&dst, const std::vector<T> &src) {
+  dst = buf.alloc<T>(src.size());
+  if (!dst) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+  if (!src.empty()) CUDA_TRY(c, cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return XCAL_OK;
+}
+template <class T>
+static int upload_c(xcal_ctx c, DevBuf &buf, const T *&dst, const std::vector<T> &src) {
+  T *d = nullptr;
+  int st = upload(c, buf, d, src);
+  dst = d;
+  return st;
+}
+#define TRY(x)              \
+  do {                      \
+    int s_ = (x);           \
+    if (s_ != XCAL_OK) return s_; \
+  } while (0)
+
+static void choose_launch(xcal_ctx c, int n) {
+  int ntiles = (n + TILE - 1) / TILE;
+  const char *m = getenv("XCAL_SYNC");
+  const char *nbv = getenv("XCAL_NBLOCKS");
+  int ns = c->ns;
+  int maxco = max_coresident_blocks(ns, c->device);
+  if (m && !strcmp(m, "block")) { c->mode = SYNC_BLOCK; c->nblocks = 1; return; }
+  if (m && !strcmp(m, "cluster")) {
+    c->mode = SYNC_CLUSTER;
+    int mc = max_cluster_blocks(ns);
+    c->nblocks = nbv ? std::max(1, std::min(mc, atoi(nbv))) : mc;
+    return;
+  }
+  if (m && !strcmp(m, "grid")) {
+    c->mode = SYNC_GRID;
+    c->nblocks = nbv ? std::max(1, std::min(maxco, atoi(nbv))) : std::max(1, maxco);
+    return;
+  }
+  if (n <= 64 * 1024) {
+    c->mode = SYNC_CLUSTER;
+    int mc = max_cluster_blocks(ns);
+    c->nblocks = std::max(1, std::min(mc, (n + TPB - 1) / TPB));
+  } else {
+    c->mode = SYNC_GRID;
+    c->nblocks = std::max(1, std::min(maxco, std::max(ntiles, 148)));
+  }
+  (void)ntiles;
+}
+
+extern "C" {
+
+int xcal_version(int *major, int *minor) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  return XCAL_OK;
+}
+
+int xcal_ctx_create(int device, uint32_t flags, xcal_ctx *out) {
+  if (!out) return XCAL_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return XCAL_ERR_CUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return XCAL_ERR_CUDA;
+  auto *c = new xcal_ctx_s();
+  c->device = device;
+  c->flags = flags;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    delete c;
+    return XCAL_ERR_CUDA;
+  }
+  *out = c;
+  return XCAL_OK;
+}
+
+int xcal_ctx_destroy(xcal_ctx c) {
+  if (!c) return XCAL_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->rbuf.release();
+  c->cbuf.release();
+  c->mbuf.release();
+  if (c->pin) cudaFreeHost(c->pin);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return XCAL_OK;
+}
+
+int xcal_last_error(xcal_ctx c, char *buf, size_t n) {
+  if (!c || !buf || !n) return XCAL_ERR_ARG;
+  snprintf(buf, n, "%s", c->err.c_str());
+  return XCAL_OK;
+}
+
+// ----------------------------------------------------------- host meshes
+int xcal_hmesh_build_unv(const char *path, double scale, xcal_hmesh *out, char *err, size_t nerr) {
+  if (!path || !out) return XCAL_ERR_ARG;
+  auto *h = new xcal_hmesh_s();
+  std::string e;
+  int st = build_unv(path, scale, h->M, e);
+  if (st) {
+    if (err && nerr) snprintf(err, nerr, "%s", e.c_str());
+    delete h;
+    return st;
+  }
+  *out = h;
+  return XCAL_OK;
+}
+
+int xcal_hmesh_counts(xcal_hmesh h, int64_t *c) {
+  if (!h || !c) return XCAL_ERR_ARG;
+  const HostMesh &M = h->M;
+  c[0] = M.nc; c[1] = M.nf; c[2] = M.nbf; c[3] = (int64_t)M.cf_face.size(); c[4] = (int64_t)M.pname.size();
+  c[5] = (int64_t)M.pfaces.size(); c[6] = M.nnodes; c[7] = (int64_t)M.names.size();
+  return XCAL_OK;
+}
+
+int xcal_hmesh_desc(xcal_hmesh h, xcal_mesh_desc *d) {
+  if (!h || !d) return XCAL_ERR_ARG;
+  HostMesh &M = h->M;
+  d->ncells = M.nc; d->nfaces = M.nf; d->nbfaces = M.nbf; d->dim = M.dim;
+  d->cell_centre = M.cc.data(); d->cell_volume = M.cvol.data();
+  d->cell_faces_ptr = M.x_cfp.data(); d->cell_faces = M.x_cf.data(); d->cell_neighbours = M.x_cn.data();
+  d->cell_nsign = M.cf_sign.data(); d->face_owner = M.x_own.data(); d->face_centre = M.fc.data();
+  d->face_normal = M.fn.data(); d->face_e = M.fe.data(); d->face_area = M.farea.data();
+  d->face_delta = M.fdelta.data(); d->face_weight = M.fweight.data();
+  d->npatches = (int64_t)M.pname.size(); d->patch_ptr = M.pptr.data(); d->patch_faces = M.x_pf.data();
+  d->patch_cells = M.x_pc.data();
+  return XCAL_OK;
+}
+
+int xcal_hmesh_patch_names(xcal_hmesh h, char *buf, size_t n) {
+  if (!h || !buf || !n) return XCAL_ERR_ARG;
+  snprintf(buf, n, "%s", h->M.names.c_str());
+  return XCAL_OK;
+}
+
+int xcal_hmesh_free(xcal_hmesh h) {
+  delete h;
+  return XCAL_OK;
+}
+
+int xcal_hmesh_from_desc(const xcal_mesh_desc *d, xcal_hmesh *out, char *err, size_t nerr) {
+  if (!d || !out) return XCAL_ERR_ARG;
+  auto *h = new xcal_hmesh_s();
+  std::string e;
+  int st = mesh_from_desc(d, h->M, e);
+  if (st) {
+    if (err && nerr) snprintf(err, nerr, "%s", e.c_str());
+    delete h;
+    return st;
+  }
+  *out = h;
+  return XCAL_OK;
+}
+
+int xcal_hmesh_renumber(xcal_hmesh m, int32_t mode, xcal_hmesh *out, int64_t *perm) {
+  if (!m || !out) return XCAL_ERR_ARG;
+  if (mode < XCAL_RENUMBER_NONE || mode > XCAL_RENUMBER_COLOR) return XCAL_ERR_ARG;
+  std::vector<int64_t> p;
+  renumber_perm(m->M, mode, p);
+  auto *h = new xcal_hmesh_s();
+  apply_perm(m->M, p, mode != XCAL_RENUMBER_NONE, h->M);
+  h->M.pname = m->M.pname;
+  h->M.prepare_export();
+  if (perm) for (size_t i = 0; i < p.size(); ++i) perm[i] = p[i] + 1;
+  *out = h;
+  return XCAL_OK;
+}
+
+int xcal_hmesh_csr(xcal_hmesh m, int64_t *nnz, int32_t *rp, int32_t *col, int32_t *fl, int32_t *bl, int32_t *nl) {
+  if (!m) return XCAL_ERR_ARG;
+  Prep P;
+  std::string e;
+  int st = prepare(m->M, P, e);
+  if (st) return st;
+  if (nnz) *nnz = P.nnz;
+  if (rp) std::copy(P.row_ptr.begin(), P.row_ptr.end(), rp);
+  if (col) std::copy(P.col.begin(), P.col.end(), col);
+  if (fl) std::copy(P.flev.begin(), P.flev.end(), fl);
+  if (bl) std::copy(P.blev.begin(), P.blev.end(), bl);
+  if (nl) { nl[0] = P.nfl; nl[1] = P.nbl; }
+  return XCAL_OK;
+}
+
+// ------------------------------------------------------------ device mesh
+int xcal_mesh_upload(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
+  if (!c) return XCAL_ERR_ARG;
+  if (renumber < XCAL_RENUMBER_NONE || renumber > XCAL_RENUMBER_COLOR) return fail(c, XCAL_ERR_ARG, "bad renumber mode");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  std::string e;
+  c->have_mesh = c->have_case = false;
+  c->cbuf.release();
+  c->rbuf.release();
+  c->mbuf.release();
+  c->run_cap = 0;
+  int st = mesh_from_desc(d, c->user, e);
+  if (st) return fail(c, st, e);
+  renumber_perm(c->user, renumber, c->perm);
+  apply_perm(c->user, c->perm, renumber != XCAL_RENUMBER_NONE, c->mesh);
+  st = prepare(c->mesh, c->prep, e);
+  if (st) return fail(c, st, e);
+  const HostMesh &M = c->mesh;
+  const Prep &P = c->prep;
+  c->ns = (M.dim == 3) ? 3 : 2;
+  KParams &h = c->hp;
+  memset(&h, 0, sizeof(h));
+  h.n = P.n; h.nf = P.nf; h.nbf = P.nbf; h.dim = M.dim; h.ntiles = (P.n + TILE - 1) / TILE;
+  std::vector<double> cx(P.n), cy(P.n), cz(P.n), fx(P.nf), fy(P.nf), fz(P.nf), nx(P.nf), ny(P.nf), nz(P.nf);
+  for (int i = 0; i < P.n; ++i) { cx[i] = M.cc[3 * i]; cy[i] = M.cc[3 * i + 1]; cz[i] = M.cc[3 * i + 2]; }
+  for (int f = 0; f < P.nf; ++f) {
+    fx[f] = M.fc[3 * f]; fy[f] = M.fc[3 * f + 1]; fz[f] = M.fc[3 * f + 2];
+    nx[f] = M.fn[3 * f]; ny[f] = M.fn[3 * f + 1]; nz[f] = M.fn[3 * f + 2];
+  }
+  DevBuf &B = c->mbuf;
+  TRY(upload_c(c, B, h.vol, M.cvol)); TRY(upload_c(c, B, h.ccx, cx)); TRY(upload_c(c, B, h.ccy, cy));
+  TRY(upload_c(c, B, h.ccz, cz)); TRY(upload_c(c, B, h.area, M.farea)); TRY(upload_c(c, B, h.delta, M.fdelta));
+  TRY(upload_c(c, B, h.wgt, M.fweight)); TRY(upload_c(c, B, h.fnx, nx)); TRY(upload_c(c, B, h.fny, ny));
+  TRY(upload_c(c, B, h.fnz, nz)); TRY(upload_c(c, B, h.fcx, fx)); TRY(upload_c(c, B, h.fcy, fy));
+  TRY(upload_c(c, B, h.fcz, fz)); TRY(upload_c(c, B, h.o1, P.o1)); TRY(upload_c(c, B, h.o2, P.o2));
+  TRY(upload_c(c, B, h.cf_ptr, P.cf_ptr)); TRY(upload_c(c, B, h.cf_face, P.cf_face));
+  TRY(upload_c(c, B, h.cf_nbr, P.cf_nbr)); TRY(upload_c(c, B, h.cf_slot, P.cf_slot));
+  TRY(upload_c(c, B, h.cf_sign, P.cf_sign)); TRY(upload_c(c, B, h.cf_first, P.cf_first));
+  TRY(upload_c(c, B, h.cb_ptr, P.cb_ptr)); TRY(upload_c(c, B, h.cb_face, P.cb_face));
+  TRY(upload_c(c, B, h.flev, P.flev)); TRY(upload_c(c, B, h.blev, P.blev));
+  TRY(upload_c(c, B, h.fl_ptr, P.fl_ptr)); TRY(upload_c(c, B, h.fl_rows, P.fl_rows));
+  TRY(upload_c(c, B, h.bl_ptr, P.bl_ptr)); TRY(upload_c(c, B, h.bl_rows, P.bl_rows));
+  h.nfl = P.nfl; h.nbl = P.nbl;
+  const int *rp, *col, *dg, *ts;
+  TRY(upload_c(c, B, rp, P.row_ptr)); TRY(upload_c(c, B, col, P.col));
+  TRY(upload_c(c, B, dg, P.diag)); TRY(upload_c(c, B, ts, P.tslot));
+  for (Mat *A : {&h.AU, &h.AP}) { A->rp = rp; A->col = col; A->diag = dg; A->tslot = ts; }
+  choose_launch(c, P.n);
+  c->have_mesh = true;
+  return XCAL_OK;
+}
+
+int xcal_mesh_permutation(xcal_ctx c, int64_t *perm, int64_t n) {
+  if (!c || !perm) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "no mesh");
+  if (n != c->user.nc) return fail(c, XCAL_ERR_ARG, "size mismatch");
+  for (int64_t i = 0; i < n; ++i) perm[i] = c->perm[i] + 1;
+  return XCAL_OK;
+}
+
+int xcal_mesh_export(xcal_ctx c, int64_t *cfp, int64_t *cf, int64_t *cn, int64_t *cs, int64_t *own,
+                     double *cc, double *cv, double *fc, double *fn, double *fe, double *fa, double *fd,
+                     double *fw, int64_t *pf, int64_t *pc) {
+  if (!c) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "no mesh");
+  const HostMesh &M = c->mesh;
+  auto cp = [](auto *dst, const auto &v) { if (dst) std::copy(v.begin(), v.end(), dst); };
+  cp(cfp, M.x_cfp); cp(cf, M.x_cf); cp(cn, M.x_cn); cp(cs, M.cf_sign); cp(own, M.x_own);
+  cp(cc, M.cc); cp(cv, M.cvol); cp(fc, M.fc); cp(fn, M.fn); cp(fe, M.fe); cp(fa, M.farea);
+  cp(fd, M.fdelta); cp(fw, M.fweight); cp(pf, M.x_pf); cp(pc, M.x_pc);
+  return XCAL_OK;
+}
+
+int xcal_mesh_csr(xcal_ctx c, int64_t *nnz, int32_t *rp, int32_t *col, int32_t *fl, int32_t *bl, int32_t *nl) {
+  if (!c) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "no mesh");
+  const Prep &P = c->prep;
+  if (nnz) *nnz = P.nnz;
+  if (rp) std::copy(P.row_ptr.begin(), P.row_ptr.end(), rp);
+  if (col) std::copy(P.col.begin(), P.col.end(), col);
+  if (fl) std::copy(P.flev.begin(), P.flev.end(), fl);
+  if (bl) std::copy(P.blev.begin(), P.blev.end(), bl);
+  if (nl) { nl[0] = P.nfl; nl[1] = P.nbl; }
+  return XCAL_OK;
+}
+
+// -------------------------------------------------------------- case setup
+static int build_bc(xcal_ctx c, DevBuf &B, const xcal_bc *bcs, int nbc, FieldBC &out,
+                    std::vector<BcEntry> &tab, bool vector, const char *what) {
+  const HostMesh &M = c->mesh;
+  int n = (int)M.nc, nbf = (int)M.nbf;
+  if (nbc < 0 || (nbc > 0 && !bcs)) return fail(c, XCAL_ERR_ARG, std::string("bad BC list for ") + what);
+  tab.assign(std::max(nbc, 1), BcEntry());
+  std::vector<int> cnt(n + 1, 0), fbc(std::max(nbf, 1), -1);
+  for (int b = 0; b < nbc; ++b) {
+    const xcal_bc &x = bcs[b];
+    if (x.patch < 0 || x.patch >= (int)M.pname.size()) return fail(c, XCAL_ERR_ARG, std::string("BC patch out of range for ") + what);
+    if (x.type < XCAL_BC_DIRICHLET || x.type > XCAL_BC_NUTWALL) return fail(c, XCAL_ERR_ARG, std::string("bad BC type for ") + what);
+    BcEntry &e = tab[b];
+    e.type = x.type; e.pad = 0;
+    for (int d = 0; d < 3; ++d) e.v[d] = vector ? x.value[d] : x.value[0];
+    e.kappa = x.kappa; e.beta1 = x.beta1; e.cmu = x.cmu; e.B = x.B; e.E = x.E;
+    for (int64_t k = M.pptr[x.patch]; k < M.pptr[x.patch + 1]; ++k) {
+      cnt[M.pcells[k] + 1]++;
+      fbc[M.pfaces[k]] = b;
+    }
+  }
+  std::vector<int> ptr(n + 1, 0);
+  for (int i = 0; i < n; ++i) ptr[i + 1] = ptr[i] + cnt[i + 1];
+  std::vector<int> face(std::max(ptr[n], 1)), bcid(std::max(ptr[n], 1));
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (int b = 0; b < nbc; ++b) {
+    const xcal_bc &x = bcs[b];
+    for (int64_t k = M.pptr[x.patch]; k < M.pptr[x.patch + 1]; ++k) {
+      int cell = (int)M.pcells[k];
+      face[fill[cell]] = (int)M.pfaces[k];
+      bcid[fill[cell]] = b;
+      fill[cell]++;
+    }
+  }
+  TRY(upload_c(c, B, out.tab, tab)); TRY(upload_c(c, B, out.a_ptr, ptr));
+  TRY(upload_c(c, B, out.a_face, face)); TRY(upload_c(c, B, out.a_bc, bcid));
+  TRY(upload_c(c, B, out.fbc, fbc));
+  return XCAL_OK;
+}
+
+static int check_solver(xcal_ctx c, const xcal_solver_cfg &s, const char *what) {
+  if (s.solver != XCAL_SOLVER_CG && s.solver != XCAL_SOLVER_BICGSTAB)
+    return fail(c, XCAL_ERR_UNSUPPORTED, std::string("solver not available for ") + what);
+  if (s.preconditioner < XCAL_PRECON_DILU || s.preconditioner > XCAL_PRECON_NONE)
+    return fail(c, XCAL_ERR_UNSUPPORTED, std::string("preconditioner not available for ") + what);
+  if (s.itmax < 0) return fail(c, XCAL_ERR_ARG, std::string("itmax < 0 for ") + what);
+  return XCAL_OK;
+}
+
+int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
+  if (!c || !cfg) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_case_setup before xcal_mesh_upload");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  if (cfg->model != XCAL_MODEL_LAMINAR) return fail(c, XCAL_ERR_UNSUPPORTED, "turbulence model not available on the device path");
+  if (cfg->precision != XCAL_PREC_FP64) return fail(c, XCAL_ERR_UNSUPPORTED, "mixed precision not available");
+  TRY(check_solver(c, cfg->solver_U, "U"));
+  TRY(check_solver(c, cfg->solver_p, "p"));
+  if (cfg->schemes_U.time == XCAL_TIME_EULER && !(cfg->dt > 0.0)) return fail(c, XCAL_ERR_ARG, "Euler time scheme needs dt > 0");
+  if (!(cfg->solver_U.relax > 0.0) || !(cfg->solver_p.relax > 0.0)) return fail(c, XCAL_ERR_ARG, "relaxation factors must be > 0");
+  c->have_case = false;
+  c->cbuf.release();
+  c->rbuf.release();
+  c->run_cap = 0;
+  KParams &h = c->hp;
+  DevBuf &B = c->cbuf;
+  int n = c->prep.n, nf = c->prep.nf, nnz = c->prep.nnz, NS = c->ns;
+  TRY(build_bc(c, B, cfg->bc_U, cfg->nbc_U, h.bcU, c->tabU, true, "U"));
+  TRY(build_bc(c, B, cfg->bc_p, cfg->nbc_p, h.bcP, c->tabP, false, "p"));
+  h.div = cfg->schemes_U.divergence; h.time = cfg->schemes_U.time; h.grad = cfg->schemes_p.gradient;
+  h.dt = cfg->dt; h.nu = cfg->nu; h.aU = cfg->solver_U.relax; h.aP = cfg->solver_p.relax;
+  h.has_pref = cfg->has_pref ? 1 : 0; h.pref = cfg->pref;
+  h.ref_cell = (int)c->perm[0];   // setReference!(p_eqn, pref, 1): the caller's first cell
+  h.kU.solver = cfg->solver_U.solver; h.kU.itmax = cfg->solver_U.itmax; h.kU.atol = cfg->solver_U.atol; h.kU.rtol = cfg->solver_U.rtol;
+  h.kP.solver = cfg->solver_p.solver; h.kP.itmax = cfg->solver_p.itmax; h.kP.atol = cfg->solver_p.atol; h.kP.rtol = cfg->solver_p.rtol;
+  h.AU.precon = cfg->solver_U.preconditioner; h.AP.precon = cfg->solver_p.preconditioner;
+  bool ok = true;
+  auto A = [&](size_t cnt) { double *p = B.alloc<double>(cnt); if (!p) ok = false; return p; };
+  h.AU.val = A(nnz); h.AU.Dpiv = A(n); h.AU.Dinv = A(n);
+  h.AP.val = A(nnz); h.AP.Dpiv = A(n); h.AP.Dinv = A(n);
+  h.U = A((size_t)n * NS); h.Uz2 = A(n); h.p = A(n); h.gp = A((size_t)n * NS); h.bU = A((size_t)n * NS);
+  h.bP = A(n); h.H = A((size_t)n * NS); h.rD = A(n); h.divH = A(n);
+  h.mdot = A(nf); h.nueff = A(nf); h.rDf = A(nf); h.pf = A(nf); h.UfH = A((size_t)nf * NS);
+  for (KWork *w : {&h.wU}) { w->x = A((size_t)n * NS); w->r = A((size_t)n * NS); w->p = A((size_t)n * NS); w->v = A((size_t)n * NS); w->s = A((size_t)n * NS); w->t = A((size_t)n * NS); w->q = A((size_t)n * NS); }
+  { KWork *w = &h.wP; w->x = A(n); w->r = A(n); w->p = A(n); w->v = A(n); w->s = A(n); w->t = A(n); w->q = A(n); }
+  h.part = A((size_t)MAXK * h.ntiles);
+  h.bar = B.alloc<Bar>(1);
+  h.done = B.alloc<int>(1);
+  if (!ok || !h.bar || !h.done) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+  // fields start at zero (ScalarField/VectorField constructors)
+  CUDA_TRY(c, cudaMemsetAsync(h.U, 0, sizeof(double) * n * NS, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.Uz2, 0, sizeof(double) * n, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.p, 0, sizeof(double) * n, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.gp, 0, sizeof(double) * n * NS, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.AU.val, 0, sizeof(double) * nnz, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.AP.val, 0, sizeof(double) * nnz, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.bU, 0, sizeof(double) * n * NS, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.bP, 0, sizeof(double) * n, c->stream));
+  if (!c->dp) {
+    c->dp = c->mbuf.alloc<KParams>(1);
+    if (!c->dp) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+  }
+  if (!c->pin || c->pin_n < (size_t)n * 3) {
+    if (c->pin) cudaFreeHost(c->pin);
+    c->pin = nullptr;
+    CUDA_TRY(c, cudaMallocHost(&c->pin, sizeof(double) * n * 3));
+    c->pin_n = (size_t)n * 3;
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->have_case = true;
+  return XCAL_OK;
+}
+
+// ------------------------------------------------------------------ fields
+static int field_target(xcal_ctx c, int32_t field, double *&base, int &stride, int &off) {
+  KParams &h = c->hp;
+  int NS = c->ns;
+  switch (field) {
+    case XCAL_FIELD_UX: base = h.U; stride = NS; off = 0; return XCAL_OK;
+    case XCAL_FIELD_UY: base = h.U; stride = NS; off = 1; return XCAL_OK;
+    case XCAL_FIELD_UZ:
+      if (NS == 3) { base = h.U; stride = 3; off = 2; } else { base = h.Uz2; stride = 1; off = 0; }
+      return XCAL_OK;
+    case XCAL_FIELD_P: base = h.p; stride = 1; off = 0; return XCAL_OK;
+    default: return fail(c, XCAL_ERR_UNSUPPORTED, "field not available on the laminar device path");
+  }
+}
+
+int xcal_field_set(xcal_ctx c, int32_t field, const double *host, int64_t n) {
+  if (!c || !host) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_field_set before xcal_case_setup");
+  if (n != c->user.nc) return fail(c, XCAL_ERR_ARG, "field size mismatch");
+  double *base; int stride, off;
+  TRY(field_target(c, field, base, stride, off));
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  double *st = c->pin;
+  for (int64_t i = 0; i < n; ++i) st[c->perm[i]] = host[i];
+  CUDA_TRY(c, cudaMemcpy2DAsync(base + off, sizeof(double) * stride, st, sizeof(double), sizeof(double), n,
+                                cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return XCAL_OK;
+}
+
+int xcal_field_get(xcal_ctx c, int32_t field, double *host, int64_t n) {
+  if (!c || !host) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_field_get before xcal_case_setup");
+  if (n != c->user.nc) return fail(c, XCAL_ERR_ARG, "field size mismatch");
+  double *base; int stride, off;
+  TRY(field_target(c, field, base, stride, off));
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  double *st = c->pin;
+  CUDA_TRY(c, cudaMemcpy2DAsync(st, sizeof(double), base + off, sizeof(double) * stride, sizeof(double), n,
+                                cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  for (int64_t i = 0; i < n; ++i) host[i] = st[c->perm[i]];
+  return XCAL_OK;
+}
+
+// -------------------------------------------------------------------- runs
+static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double *Ruy, double *Ruz,
+                       double *Rp, int32_t *kry, int32_t *done) {
+  if (!c) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "run before xcal_case_setup");
+  if (iters < 0) return fail(c, XCAL_ERR_ARG, "iterations < 0");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  KParams &h = c->hp;
+  if (iters > c->run_cap) {
+    c->rbuf.release();
+    h.R = c->rbuf.alloc<double>((size_t)iters * 4);
+    h.kry = c->rbuf.alloc<int>((size_t)iters * 5);
+    if (!h.R || !h.kry) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+    c->run_cap = iters;
+  }
+  std::vector<double> ones((size_t)std::max(iters, 1) * 4, 1.0);
+  CUDA_TRY(c, cudaMemcpyAsync(h.R, ones.data(), sizeof(double) * iters * 4, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.kry, 0, sizeof(int) * iters * 5, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(h.done, 0, sizeof(int), c->stream));
+  h.mode = c->mode;
+  CUDA_TRY(c, cudaMemcpyAsync(c->dp, &h, sizeof(KParams), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+  if (iters > 0) CUDA_TRY(c, launch_program(c->ns, c->mode, c->nblocks, c->dp, prog, iters, c->stream));
+  CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_ms = ms;
+  Bar bar;
+  int dn = 0;
+  CUDA_TRY(c, cudaMemcpy(&bar, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, cudaMemcpy(&dn, h.done, sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<double> R((size_t)std::max(iters, 1) * 4);
+  std::vector<int> K((size_t)std::max(iters, 1) * 5);
+  if (iters > 0) {
+    CUDA_TRY(c, cudaMemcpy(R.data(), h.R, sizeof(double) * iters * 4, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, cudaMemcpy(K.data(), h.kry, sizeof(int) * iters * 5, cudaMemcpyDeviceToHost));
+  }
+  for (int i = 0; i < iters; ++i) {
+    if (Rux) Rux[i] = R[4 * i];
+    if (Ruy) Ruy[i] = R[4 * i + 1];
+    if (Ruz) Ruz[i] = R[4 * i + 2];
+    if (Rp) Rp[i] = R[4 * i + 3];
+  }
+  if (kry) std::copy(K.begin(), K.begin() + (size_t)iters * 5, kry);
+  if (done) *done = dn;
+  if (bar.err) return fail(c, XCAL_ERR_TIMEOUT, "device barrier timed out");
+  return XCAL_OK;
+}
+
+int xcal_simple_run(xcal_ctx c, int32_t iters, double *Rux, double *Ruy, double *Ruz, double *Rp,
+                    int32_t *kry, int32_t *done) {
+  return run_program(c, PROG_SIMPLE, iters, Rux, Ruy, Ruz, Rp, kry, done);
+}
+
+int xcal_piso_run(xcal_ctx c, int32_t iters, double *Rux, double *Ruy, double *Ruz, double *Rp,
+                  int32_t *kry, int32_t *done) {
+  return run_program(c, PROG_PISO, iters, Rux, Ruy, Ruz, Rp, kry, done);
+}
+
+int xcal_last_run_stats(xcal_ctx c, double *ms, double *phase, int32_t nph) {
+  if (!c) return XCAL_ERR_ARG;
+  if (ms) *ms = c->last_ms;
+  for (int i = 0; phase && i < nph; ++i) phase[i] = 0.0;
+  return XCAL_OK;
+}
+
+int xcal_equation_get(xcal_ctx c, int32_t which, double *vals, double *b0, double *b1, double *b2) {
+  if (!c) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "no case");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const KParams &h = c->hp;
+  int n = c->prep.n, nnz = c->prep.nnz, NS = c->ns;
+  if (which == 0) {
+    if (vals) CUDA_TRY(c, cudaMemcpy(vals, h.AU.val, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+    std::vector<double> b((size_t)n * NS);
+    CUDA_TRY(c, cudaMemcpy(b.data(), h.bU, sizeof(double) * n * NS, cudaMemcpyDeviceToHost));
+    double *dst[3] = {b0, b1, b2};
+    for (int d = 0; d < NS; ++d)
+      if (dst[d]) for (int i = 0; i < n; ++i) dst[d][i] = b[(size_t)i * NS + d];
+    return XCAL_OK;
+  }
+  if (which == 1) {
+    if (vals) CUDA_TRY(c, cudaMemcpy(vals, h.AP.val, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+    if (b0) CUDA_TRY(c, cudaMemcpy(b0, h.bP, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return XCAL_OK;
+  }
+  return fail(c, XCAL_ERR_ARG, "which must be 0 (momentum) or 1 (pressure)");
+}
+
+// -------------------------------------------------------- standalone solve
+int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, const int32_t *row_ptr,
+                      const int32_t *col, const double *val, const double *b, double *x, int32_t itmax,
+                      double atol, double rtol, int32_t *niter, double *final_rnorm) {
+  if (!c || !row_ptr || !col || !val || !b || !x || n64 <= 0 || n64 > (1 << 30)) return XCAL_ERR_ARG;
+  if (solver != XCAL_SOLVER_CG && solver != XCAL_SOLVER_BICGSTAB) return fail(c, XCAL_ERR_UNSUPPORTED, "solver");
+  if (precon < XCAL_PRECON_DILU || precon > XCAL_PRECON_NONE) return fail(c, XCAL_ERR_UNSUPPORTED, "preconditioner");
+  if (itmax < 0) return fail(c, XCAL_ERR_ARG, "itmax < 0");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  int n = (int)n64;
+  if (row_ptr[0] != 0) return fail(c, XCAL_ERR_ARG, "row_ptr[0] must be 0");
+  for (int i = 0; i < n; ++i) {
+    if (row_ptr[i + 1] < row_ptr[i]) return fail(c, XCAL_ERR_ARG, "row_ptr not monotone");
+    for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+      if (col[k] < 0 || col[k] >= n) return fail(c, XCAL_ERR_ARG, "column out of range");
+      if (k > row_ptr[i] && col[k] <= col[k - 1]) return fail(c, XCAL_ERR_ARG, "columns not strictly ascending");
+    }
+  }
+  int nnz = row_ptr[n];
+  std::vector<int> rp(row_ptr, row_ptr + n + 1), cl(col, col + nnz), dg(n, -1), ts(nnz, -1);
+  auto find = [&](int r, int cc) -> int {
+    auto bb = cl.begin() + rp[r], ee = cl.begin() + rp[r + 1];
+    auto it = std::lower_bound(bb, ee, cc);
+    return (it != ee && *it == cc) ? (int)(it - cl.begin()) : -1;
+  };
+  for (int i = 0; i < n; ++i) {
+    dg[i] = find(i, i);
+    if (dg[i] < 0) return fail(c, XCAL_ERR_ARG, "missing diagonal entry");
+  }
+  for (int r = 0; r < n; ++r)
+    for (int k = rp[r]; k < rp[r + 1]; ++k) {
+      ts[k] = find(cl[k], r);
+      if (ts[k] < 0) return fail(c, XCAL_ERR_ARG, "pattern not symmetric");
+    }
+  std::vector<int> fl(n, 0), bl(n, 0);
+  for (int i = 0; i < n; ++i) { int l = 0; for (int k = rp[i]; k < dg[i]; ++k) l = std::max(l, fl[cl[k]] + 1); fl[i] = l; }
+  for (int i = n - 1; i >= 0; --i) { int l = 0; for (int k = dg[i] + 1; k < rp[i + 1]; ++k) l = std::max(l, bl[cl[k]] + 1); bl[i] = l; }
+  auto bucket = [&](const std::vector<int> &lev, std::vector<int> &ptr, std::vector<int> &rows, int &nl) {
+    nl = 0;
+    for (int i = 0; i < n; ++i) nl = std::max(nl, lev[i] + 1);
+    ptr.assign(nl + 1, 0);
+    for (int i = 0; i < n; ++i) ptr[lev[i] + 1]++;
+    for (int l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
+    rows.resize(n);
+    std::vector<int> f(ptr.begin(), ptr.end() - 1);
+    for (int i = 0; i < n; ++i) rows[f[lev[i]]++] = i;
+  };
+  std::vector<int> flp, flr, blp, blr;
+  int nfl, nbl;
+  bucket(fl, flp, flr, nfl);
+  bucket(bl, blp, blr, nbl);
+  DevBuf B;
+  KParams h;
+  memset(&h, 0, sizeof(h));
+  h.n = n; h.ntiles = (n + TILE - 1) / TILE;
+  TRY(upload_c(c, B, h.flev, fl)); TRY(upload_c(c, B, h.blev, bl));
+  TRY(upload_c(c, B, h.fl_ptr, flp)); TRY(upload_c(c, B, h.fl_rows, flr));
+  TRY(upload_c(c, B, h.bl_ptr, blp)); TRY(upload_c(c, B, h.bl_rows, blr));
+  h.nfl = nfl; h.nbl = nbl;
+  TRY(upload_c(c, B, h.AU.rp, rp)); TRY(upload_c(c, B, h.AU.col, cl));
+  TRY(upload_c(c, B, h.AU.diag, dg)); TRY(upload_c(c, B, h.AU.tslot, ts));
+  std::vector<double> vv(val, val + nnz), bb(b, b + n), xx(x, x + n);
+  TRY(upload(c, B, h.AU.val, vv));
+  TRY(upload(c, B, h.sb, bb));
+  TRY(upload(c, B, h.U, xx));
+  h.AU.precon = precon;
+  bool ok = true;
+  auto A = [&](size_t cnt) { double *p = B.alloc<double>(cnt); if (!p) ok = false; return p; };
+  h.AU.Dpiv = A(n); h.AU.Dinv = A(n);
+  KWork &w = h.wU;
+  w.x = A(n); w.r = A(n); w.p = A(n); w.v = A(n); w.s = A(n); w.t = A(n); w.q = A(n);
+  h.part = A((size_t)MAXK * h.ntiles);
+  h.solve_out = A(2);
+  h.bar = B.alloc<Bar>(1);
+  h.done = B.alloc<int>(1);
+  KParams *dp = B.alloc<KParams>(1);
+  if (!ok || !h.bar || !h.done || !dp) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+  h.solve_solver = solver; h.solve_itmax = itmax; h.solve_atol = atol; h.solve_rtol = rtol;
+  int mode, nb;
+  {
+    int saved_ns = c->ns, saved_mode = c->mode, saved_nb = c->nblocks;
+    c->ns = 1;
+    choose_launch(c, n);
+    mode = c->mode; nb = c->nblocks;
+    c->ns = saved_ns; c->mode = saved_mode; c->nblocks = saved_nb;
+  }
+  h.mode = mode;
+  CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(dp, &h, sizeof(KParams), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, launch_program(1, mode, nb, dp, PROG_SOLVE, 1, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  Bar bar;
+  double so[2];
+  CUDA_TRY(c, cudaMemcpy(&bar, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, cudaMemcpy(so, h.solve_out, sizeof(so), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, cudaMemcpy(x, h.U, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (niter) *niter = (int32_t)so[0];
+  if (final_rnorm) *final_rnorm = so[1];
+  if (bar.err) return fail(c, XCAL_ERR_TIMEOUT, "device barrier timed out");
+  return XCAL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+"""The benchmark configurations as ready-made cases (mesh, model, config, pref).
+
+    cavity2d   lid-driven cavity 0.1 m, n x n quads, Re=100 (lid 1 m/s, nu=1e-3)
+    bfs        laminar backward-facing step h=10 mm, 27 cells/h (47,385 cells),
+               graded 1.05, jittered +-10% (seed 20240101), inlet 0.5 m/s, nu=1e-4
+    cavity3d   unit cube n^3 hexahedra, lid y=1 at (1,0,0), nu=1e-3
+
+Schemes and solvers follow the configurations: divergence Upwind, Laplacian
+Linear, gradient Orthogonal, steady; U relax 0.7, p relax 0.3; p CG+DILU and U
+BiCGSTAB+DILU with itmax 100, atol sqrt(eps), rtol 1e-3.
+"""
+import os
+import tempfile
+
+import numpy as np
+
+from . import api as X
+from . import meshgen
+from .mesh import Mesh2
+
+_CACHE = os.environ.get("XCAL_MESH_CACHE", os.path.join(tempfile.gettempdir(), "xcal_meshes"))
+
+
+def _unv(name, writer, **kw):
+    os.makedirs(_CACHE, exist_ok=True)
+    key = "_".join(f"{k}{v}" for k, v in sorted(kw.items()))
+    path = os.path.join(_CACHE, f"{name}_{key}.unv")
+    if not os.path.exists(path):
+        tmp = path + f".{os.getpid()}.tmp"
+        writer(tmp, **kw)
+        os.replace(tmp, path)
+    return path
+
+
+def solvers_for(model, p_solver=X.CgSolver, u_solver=X.BicgstabSolver, precon=X.DILU,
+                relax_u=0.7, relax_p=0.3, itmax=100):
+    return dict(
+        U=X.set_solver(model.U, solver=u_solver, preconditioner=precon(), convergence=1e-7,
+                       relax=relax_u, itmax=itmax),
+        p=X.set_solver(model.p, solver=p_solver, preconditioner=precon(), convergence=1e-7,
+                       relax=relax_p, itmax=itmax))
+
+
+def cavity2d(n=40, iterations=1000, divergence=X.Upwind, gradient=X.Orthogonal, **kw):
+    path = _unv("cavity", meshgen.cavity_unv, n=n, L=0.1)
+    mesh = X.build_mesh(path)
+    model = X.RANS(X.Laminar, mesh=mesh, viscosity=X.ConstantScalar(1e-3))
+    X.assign(model, "U", X.Dirichlet("inlet", [0.0, 0.0, 0.0]), X.Dirichlet("outlet", [0.0, 0.0, 0.0]),
+             X.Dirichlet("bottom", [0.0, 0.0, 0.0]), X.Dirichlet("top", [1.0, 0.0, 0.0]))
+    X.assign(model, "p", *[X.Neumann(b, 0.0) for b in ("inlet", "outlet", "bottom", "top")])
+    schemes = dict(U=X.set_schemes(divergence=divergence, gradient=gradient),
+                   p=X.set_schemes(divergence=divergence, gradient=gradient))
+    config = X.Configuration(solvers=solvers_for(model, **kw), schemes=schemes,
+                             runtime=X.set_runtime(iterations=iterations, write_interval=-1, time_step=1))
+    X.initialise(model.U, [0.0, 0.0, 0.0])
+    X.initialise(model.p, 0.0)
+    return mesh, model, config, 0.0
+
+
+def bfs(cells_per_h=27, iterations=2000, divergence=X.Upwind, gradient=X.Orthogonal, **kw):
+    path = _unv("bfs", meshgen.bfs_unv, cells_per_h=cells_per_h)
+    mesh = X.build_mesh(path)
+    model = X.RANS(X.Laminar, mesh=mesh, viscosity=X.ConstantScalar(1e-4))
+    X.assign(model, "U", X.Dirichlet("inlet", [0.5, 0.0, 0.0]), X.Neumann("outlet", 0.0),
+             X.Dirichlet("wall", [0.0, 0.0, 0.0]), X.Dirichlet("top", [0.0, 0.0, 0.0]))
+    X.assign(model, "p", X.Neumann("inlet", 0.0), X.Dirichlet("outlet", 0.0), X.Neumann("wall", 0.0),
+             X.Neumann("top", 0.0))
+    schemes = dict(U=X.set_schemes(divergence=divergence, gradient=gradient),
+                   p=X.set_schemes(divergence=divergence, gradient=gradient))
+    config = X.Configuration(solvers=solvers_for(model, **kw), schemes=schemes,
+                             runtime=X.set_runtime(iterations=iterations, write_interval=-1, time_step=1))
+    X.initialise(model.U, [0.0, 0.0, 0.0])
+    X.initialise(model.p, 0.0)
+    return mesh, model, config, None
+
+
+def cavity3d(n=128, iterations=500, **kw):
+    m = meshgen.hex_cavity(n)
+    mesh = Mesh2.from_dict(m)
+    model = X.RANS(X.Laminar, mesh=mesh, viscosity=X.ConstantScalar(1e-3))
+    walls = ("xmin", "xmax", "ymin", "zmin", "zmax")
+    X.assign(model, "U", *[X.Dirichlet(w, [0.0, 0.0, 0.0]) for w in walls],
+             X.Dirichlet("lid", [1.0, 0.0, 0.0]))
+    X.assign(model, "p", *[X.Neumann(w, 0.0) for w in walls + ("lid",)])
+    schemes = dict(U=X.set_schemes(divergence=X.Upwind), p=X.set_schemes(divergence=X.Upwind))
+    config = X.Configuration(solvers=solvers_for(model, **kw), schemes=schemes,
+                             runtime=X.set_runtime(iterations=iterations, write_interval=-1, time_step=1))
+    X.initialise(model.U, [0.0, 0.0, 0.0])
+    X.initialise(model.p, 0.0)
+    return mesh, model, config, 0.0
+
+
+def fields(model):
+    n = model.mesh.ncells
+    U = np.stack([model.U.x.values, model.U.y.values, model.U.z.values])
+    return U.reshape(3, n).copy(), model.p.values.copy()
