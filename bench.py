@@ -1,0 +1,352 @@
+"""Benchmark: SIMPLE cell-iterations/s of the laminar backward-facing step
+(47,385 cells, FP64, CG+DILU for p, BiCGSTAB+DILU for U) on the device path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xcal|reference]
+                    [--config bfs|cavity|cavity3d] [--renumber color|rcm|none]
+
+A step is one SIMPLE iteration of the case (one launch of the persistent device
+program).  Steps run from zero initial fields, as the case does; L2 is flushed
+between steps (a 256 MiB write), and each step is timed with CUDA events on the
+library's stream.  N > 1 runs N independent replicas (one per rank, weak
+scaling): a single case does not shard, there is no collective on the data path.
+
+--impl reference times the CPU restatement of the reference (single thread, as
+the reference) on the same case and prints the same metric.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "xcalibre_tw.jl_b200"))
+
+METRIC = "SIMPLE cell-iters/s"
+UNIT = "cell-iters/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="xcal", choices=["xcal", "reference"])
+    ap.add_argument("--config", default="bfs", choices=["bfs", "cavity", "cavity3d"])
+    ap.add_argument("--renumber", default="color", choices=["color", "rcm", "none"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-flush", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def build_case(name):
+    from xcal import cases
+    if name == "bfs":
+        mesh, model, config, pref = cases.bfs(27, iterations=2000)
+        desc = "laminar backward-facing step h=10mm, 27 cells/h, graded 1.05, jittered 10%, Re=50"
+    elif name == "cavity":
+        mesh, model, config, pref = cases.cavity2d(40, iterations=1000)
+        desc = "2D lid-driven cavity 40x40, Re=100"
+    else:
+        mesh, model, config, pref = cases.cavity3d(128, iterations=500)
+        desc = "3D lid-driven cavity 128^3 hexahedra, Re=1000"
+    return mesh, model, config, pref, desc
+
+
+# ------------------------------------------------------------ byte model
+def algorithmic_bytes(mesh, kry, ns):
+    """Algorithmic HBM bytes of one SIMPLE iteration given its Krylov counts
+    (U iterations per component, p iterations).  Per-operation figures:
+      SpMV (CSR, k vectors)   nnz*(s+4) + (N+1)*4 + 2*k*N*s
+      DILU apply (k vectors)  2*Fi*(s+4) + 2*N*s + 4*k*N*s
+      DILU update             Fi*(2s+4) + 2*N*s
+      vector kernels          (vectors read + written) * N * s
+      assembly (k RHS)        Fi*(8+6s) + N*(5s + 3s*(k-1)) + Fb*(4+4s)
+      face fields             face arrays * F * s + gathered cell arrays * N * s
+    """
+    s = 8
+    N = mesh.ncells
+    F = mesh.nfaces
+    Fb = mesh.nbfaces
+    Fi = F - Fb
+    nnz = N + 2 * Fi
+
+    def spmv(k):
+        return nnz * (s + 4) + (N + 1) * 4 + 2 * k * N * s
+
+    def dilu(k):
+        return 2 * Fi * (s + 4) + 2 * N * s + 4 * k * N * s
+    dilu_upd = Fi * (2 * s + 4) + 2 * N * s
+    vec = N * s
+    itU = int(max(kry[:ns]))
+    itP = int(kry[3])
+    b = 0
+    # momentum: assembly, r0 = b - A x0, DILU update + first apply, BiCGSTAB init
+    b += Fi * (8 + 6 * s) + N * (5 * s + 3 * s * (ns - 1)) + Fb * (4 + 4 * s)
+    b += spmv(ns) + dilu_upd + dilu(ns) + 3 * ns * vec
+    b += itU * (2 * spmv(ns) + 2 * dilu(ns) + 20 * ns * vec)
+    b += 3 * ns * vec                                    # x + x0
+    b += spmv(ns) + (2 + 2) * ns * vec + N * (s + 4)     # residual!, remove_pressure_source!, H!
+    b += F * s * (1 + ns) + (1 + ns) * N * s + F * 8     # rDf, Uf(H) face interpolation
+    # pressure: div!, assembly, CG
+    b += F * s * ns + N * 2 * s + Fi * (8 + 4 * s) + N * 3 * s
+    b += spmv(1) + dilu_upd + dilu(1) + 3 * vec
+    b += itP * (spmv(1) + dilu(1) + 13 * vec)
+    b += 3 * vec + spmv(1) + 2 * vec                     # relax, residual!
+    b += F * s + 2 * N * s                               # pf interpolation
+    b += Fi * (8 + 2 * s) + N * s * (1 + ns * 3)         # Green-Gauss + correct_velocity!
+    b += F * s * (1 + 3) + ns * N * s                    # Uf(U), flux!
+    return b
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        mx = float(rows[0][2])
+        reasons = set()
+        for r in rows:
+            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def load_peaks():
+    try:
+        m = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(workload_key):
+    try:
+        t = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        return t.get(workload_key)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- CPU oracle
+def cpu_oracle_rate(mesh, model, config, pref, seconds):
+    """Single-threaded CPU restatement of the reference on the same case: time
+    SIMPLE iterations from the start of the run until the budget is used."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import xcal as X
+    from xcal import cases
+    om = O.from_mesh2(mesh)
+    case, keep = X.make_case(model, config, pref)
+    U, p = cases.fields(model)
+    t0 = time.perf_counter()
+    O.run(om, case, 2, U, p)                 # estimate
+    per = (time.perf_counter() - t0) / 2
+    its = max(2, min(2000, int(seconds / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    out = O.run(om, case, its, U, p)
+    dt = time.perf_counter() - t0
+    its_done = out["done"]
+    return mesh.ncells * its_done / dt, its_done, dt
+
+
+def cpu_model():
+    try:
+        for l in open("/proc/cpuinfo"):
+            if l.startswith("model name"):
+                return l.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+# -------------------------------------------------------------------- main
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    mesh, model, config, pref, desc = build_case(a.config)
+    N = mesh.ncells
+    workload = f"{a.config}_{N}_fp64_simple"
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        steps = a.steps
+        rate, its, dt = cpu_oracle_rate(mesh, model, config, pref, seconds=min(120.0, max(5.0, a.cpu_seconds)))
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": a.gpus,
+                "steps": its, "warmup": 0, "ms_per_step": 1000 * dt / its, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic mesh from the seeded generator (reference UNV construction rules)",
+                "config": {"workload": desc, "cells": N, "renumber": "none (reference order)"},
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                                 "sample": f"first {its} SIMPLE iterations of the case ({dt:.1f} s), "
+                                           f"CPU: {cpu_model()}"},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    import xcal as X
+    from xcal import _abi, cases
+
+    renum = {"color": _abi.RENUMBER_COLOR, "rcm": _abi.RENUMBER_RCM, "none": _abi.RENUMBER_NONE}[a.renumber]
+    case, keep = X.make_case(model, config, pref)
+    s = X.Solver(mesh, device=local if world > 1 else 0, renumber=renum)
+    s.setup(case)
+    U0, p0 = cases.fields(model)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    flush = None if a.no_flush else torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def reset():
+        for f, v in ((_abi.FIELD_UX, U0[0]), (_abi.FIELD_UY, U0[1]), (_abi.FIELD_UZ, U0[2]), (_abi.FIELD_P, p0)):
+            s.set_field(f, v)
+
+    def do_flush():
+        if flush is not None:
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+
+    # warm-up (untimed), then restart the case from its initial fields
+    reset()
+    for _ in range(max(a.warmup, 0)):
+        s.run(1, want_krylov=False)
+    reset()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ms = []
+    kry = []
+    gpu_index = local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)
+    with ClockSampler(gpu_index) as clk:
+        for k in range(a.steps):
+            do_flush()
+            out = s.run(1)
+            ms.append(s.last_ms())
+            kry.append(out["krylov"][0])
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    total_ms = float(sum(ms))
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * N * a.steps / (total_ms / 1000.0)
+    kry = np.array(kry)
+    # roofline of the (single) device program kernel
+    ns = 3 if mesh.dim == 3 else 2
+    bytes_per_step = np.array([algorithmic_bytes(mesh, kr, ns) for kr in kry], dtype=np.float64)
+    achieved_gbs = float(bytes_per_step.sum() / (np.array(ms).sum() / 1000.0) / 1e9)
+    peak, peak_kind = load_peaks()
+
+    # end to end through the public API with host buffers
+    e2e_steps = a.e2e_steps or min(a.steps, 100)
+    reset()
+    Uh = [U0[0].copy(), U0[1].copy()]
+    ph = p0.copy()
+    e2e_t = 0.0
+    for k in range(e2e_steps):
+        do_flush()
+        t0 = time.perf_counter()
+        s.set_field(_abi.FIELD_UX, Uh[0]); s.set_field(_abi.FIELD_UY, Uh[1]); s.set_field(_abi.FIELD_P, ph)
+        out = s.run(1, want_krylov=False)
+        Uh[0] = s.get_field(_abi.FIELD_UX); Uh[1] = s.get_field(_abi.FIELD_UY); ph = s.get_field(_abi.FIELD_P)
+        e2e_t += time.perf_counter() - t0
+    e2e_value = world * N * e2e_steps / e2e_t
+    if dist:
+        t = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = world * N * e2e_steps / float(t.item())
+    h2d = 3 * N * 8
+    d2h = 3 * N * 8 + 4 * 8 + 5 * 4
+    s.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        rate, its, dt = cpu_oracle_rate(mesh, model, config, pref, a.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"CPU oracle, first {its} SIMPLE iterations of the same case ({dt:.1f} s), "
+                         f"1 thread, {cpu_model()}"}
+    clocks = clk.summary()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic mesh from the seeded generator (reference UNV construction rules)",
+        "config": {"workload": desc, "cells": N, "renumber": a.renumber,
+                   "step": "one SIMPLE iteration from zero initial fields",
+                   "l2": "flushed between steps (256 MiB write)" if flush is not None else "not flushed",
+                   "krylov_mean": {"U": float(kry[:, 0].mean()), "p": float(kry[:, 3].mean())},
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": achieved_gbs / peak, "peak_kind": peak_kind,
+                     "traffic": load_traffic(workload),
+                     "kernel": "xcal_program_kernel (persistent SIMPLE iteration)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "gpu_launches": a.steps,
+        "clocks": clocks,
+        "impl": "xcal",
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

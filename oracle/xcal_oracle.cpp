@@ -72,10 +72,10 @@ static inline double jmax(double a, double b) {
 }
 
 // ------------------------------------------------------- canonical reduction
-// Fixed-tree sum: tiles of 1024 values; 256 lanes x 4 strided values per lane,
-// a warp shuffle-down tree (offsets 16,8,4,2,1), then an 8-way tree over the
-// warps.  Tile partials are folded the same way (lane t sums partials t,
-// t+256, ... sequentially).  The device reduction kernels follow this order.
+// Fixed-tree sum: tiles of 256 values (one per lane); inside a tile a warp
+// shuffle-down tree (offsets 16,8,4,2,1) then an 8-way tree over the warps.
+// Tile partials are folded the same way (lane t sums partials t, t+256, ...
+// sequentially, then the same tree).  The device reductions follow this order.
 static double canon_tree256(double *w) {
   double ws[8];
   for (int wp = 0; wp < 8; ++wp) {
@@ -92,18 +92,13 @@ static double canon_tree256(double *w) {
 
 template <class F>
 static double canon_sum_f(i64 n, F f) {
-  i64 ntiles = (n + 1023) / 1024;
+  i64 ntiles = (n + 255) / 256;
   std::vector<double> part(ntiles);
   double w[256];
   for (i64 t = 0; t < ntiles; ++t) {
     for (int l = 0; l < 256; ++l) {
-      double s = 0.0;
-      for (int m = 0; m < 4; ++m) {
-        i64 e = t * 1024 + m * 256 + l;
-        double v = (e < n) ? f(e) : 0.0;
-        s = (m == 0) ? v : s + v;
-      }
-      w[l] = s;
+      i64 e = t * 256 + l;
+      w[l] = (e < n) ? f(e) : 0.0;
     }
     part[t] = canon_tree256(w);
   }

@@ -539,20 +539,49 @@ int prepare(const HostMesh &M, Prep &P, std::string &err) {
       P.tslot[k] = find(P.col[k], r);
       if (P.tslot[k] < 0) { err = "matrix pattern not symmetric"; return XCAL_ERR_MESH; }
     }
-  // cell -> internal face entries with their CSR slots
-  int tot = (int)M.cf_ptr[n];
-  P.cf_ptr.resize(n + 1); P.cf_face.resize(tot); P.cf_nbr.resize(tot); P.cf_slot.resize(tot);
-  P.cf_sign.resize(tot); P.cf_first.resize(tot);
-  for (int c = 0; c <= n; ++c) P.cf_ptr[c] = (int)M.cf_ptr[c];
-  for (int c = 0; c < n; ++c)
-    for (int k = P.cf_ptr[c]; k < P.cf_ptr[c + 1]; ++k) {
-      P.cf_face[k] = (int)M.cf_face[k]; P.cf_nbr[k] = (int)M.cf_nbr[k];
-      P.cf_sign[k] = (signed char)M.cf_sign[k];
-      P.cf_slot[k] = find(c, (int)M.cf_nbr[k]);
-      bool first = true;
-      for (int q = P.cf_ptr[c]; q < k; ++q) if (P.cf_slot[q] == P.cf_slot[k]) first = false;
-      P.cf_first[k] = first ? 1 : 0;
+  // ELL layout of the matrix
+  P.np = ((n + 255) / 256) * 256;
+  P.W = 0;
+  for (int i = 0; i < n; ++i) P.W = std::max(P.W, P.row_ptr[i + 1] - P.row_ptr[i]);
+  if (P.W > 64) { err = "more than 63 neighbours in one cell"; return XCAL_ERR_UNSUPPORTED; }
+  P.e_col.assign((size_t)P.W * P.np, -1);
+  P.e_tpos.assign((size_t)P.W * P.np, -1);
+  P.dpos.assign(P.np, 0);
+  P.csr2ell.assign(P.nnz, 0);
+  for (int i = 0; i < n; ++i)
+    for (int k = P.row_ptr[i]; k < P.row_ptr[i + 1]; ++k) {
+      int e = (k - P.row_ptr[i]) * P.np + i;
+      P.e_col[e] = P.col[k];
+      P.csr2ell[k] = e;
     }
+  for (int i = 0; i < n; ++i) {
+    P.dpos[i] = P.csr2ell[P.diag[i]];
+    for (int k = P.row_ptr[i]; k < P.row_ptr[i + 1]; ++k) P.e_tpos[P.csr2ell[k]] = P.csr2ell[P.tslot[k]];
+  }
+  // cell -> internal face entries (reference order) with their matrix positions
+  P.Wf = 0;
+  for (int c = 0; c < n; ++c) P.Wf = std::max(P.Wf, (int)(M.cf_ptr[c + 1] - M.cf_ptr[c]));
+  P.Wf = std::max(P.Wf, 1);
+  P.f_face.assign((size_t)P.Wf * P.np, -1);
+  P.f_nbr.assign((size_t)P.Wf * P.np, 0);
+  P.f_pos.assign((size_t)P.Wf * P.np, 0);
+  P.f_sign.assign((size_t)P.Wf * P.np, 0);
+  P.f_first.assign((size_t)P.Wf * P.np, 0);
+  for (int c = 0; c < n; ++c) {
+    int b = (int)M.cf_ptr[c];
+    for (int k = b; k < (int)M.cf_ptr[c + 1]; ++k) {
+      int e = (k - b) * P.np + c;
+      int nb = (int)M.cf_nbr[k];
+      int slot = find(c, nb);
+      P.f_face[e] = (int)M.cf_face[k];
+      P.f_nbr[e] = nb;
+      P.f_pos[e] = P.csr2ell[slot];
+      P.f_sign[e] = (signed char)M.cf_sign[k];
+      bool first = true;
+      for (int q = b; q < k; ++q) if (M.cf_nbr[q] == nb) first = false;
+      P.f_first[e] = first ? 1 : 0;
+    }
+  }
   // boundary faces of each cell in face-id order
   std::vector<int> bc_cnt(n + 1, 0);
   for (int f = 0; f < P.nbf; ++f) bc_cnt[M.o1[f] + 1]++;
@@ -575,18 +604,10 @@ int prepare(const HostMesh &M, Prep &P, std::string &err) {
     for (int k = P.diag[i] + 1; k < P.row_ptr[i + 1]; ++k) l = std::max(l, P.blev[P.col[k]] + 1);
     P.blev[i] = l;
   }
-  auto bucket = [&](const std::vector<int> &lev, std::vector<int> &ptr, std::vector<int> &rows, int &nl) {
-    nl = 0;
-    for (int i = 0; i < n; ++i) nl = std::max(nl, lev[i] + 1);
-    ptr.assign(nl + 1, 0);
-    for (int i = 0; i < n; ++i) ptr[lev[i] + 1]++;
-    for (int l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
-    rows.resize(n);
-    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-    for (int i = 0; i < n; ++i) rows[fill[lev[i]]++] = i;
-  };
-  bucket(P.flev, P.fl_ptr, P.fl_rows, P.nfl);
-  bucket(P.blev, P.bl_ptr, P.bl_rows, P.nbl);
+  P.nfl = P.nbl = 1;
+  for (int i = 0; i < n; ++i) { P.nfl = std::max(P.nfl, P.flev[i] + 1); P.nbl = std::max(P.nbl, P.blev[i] + 1); }
+  P.flev.resize(P.np, 0);
+  P.blev.resize(P.np, 0);
   P.o1.resize(nf); P.o2.resize(nf);
   for (int f = 0; f < nf; ++f) { P.o1[f] = (int)M.o1[f]; P.o2[f] = (int)M.o2[f]; }
   return XCAL_OK;

@@ -34,15 +34,19 @@ void renumber_perm(const HostMesh &M, int mode, std::vector<int64_t> &perm);
 void apply_perm(const HostMesh &in, const std::vector<int64_t> &perm, bool reorder_faces,
                 HostMesh &out);
 
-// Device-ready integer structures built from a (renumbered) mesh.
+// Device-ready integer structures built from a (renumbered) mesh.  Matrix and
+// per-cell face lists use an ELL layout padded to np = 256*ceil(n/256) rows:
+// entry k of row i sits at k*np + i (coalesced across a warp); unused entries
+// hold column -1.  Entries of a row are in ascending column order.
 struct Prep {
-  int n = 0, nf = 0, nbf = 0, nnz = 0;
-  std::vector<int> row_ptr, col, diag, tslot;
-  std::vector<int> cf_ptr, cf_face, cf_nbr, cf_slot;
-  std::vector<signed char> cf_sign;
-  std::vector<unsigned char> cf_first;
+  int n = 0, nf = 0, nbf = 0, nnz = 0, np = 0, W = 0, Wf = 0;
+  std::vector<int> row_ptr, col, diag, tslot;   // CSR view (export, tests)
+  std::vector<int> e_col, e_tpos, dpos, csr2ell;
+  std::vector<int> f_face, f_nbr, f_pos;
+  std::vector<signed char> f_sign;
+  std::vector<unsigned char> f_first;
   std::vector<int> cb_ptr, cb_face;          // boundary faces per cell, face-id order
-  std::vector<int> flev, blev, fl_ptr, fl_rows, bl_ptr, bl_rows;
+  std::vector<int> flev, blev;
   int nfl = 0, nbl = 0;
   std::vector<int> o1, o2;
 };

@@ -113,13 +113,15 @@ static void choose_launch(xcal_ctx c, int n) {
     c->nblocks = nbv ? std::max(1, std::min(maxco, atoi(nbv))) : std::max(1, maxco);
     return;
   }
-  if (n <= 64 * 1024) {
+  // One CTA per 256-row tile: a hardware cluster barrier while the tiles fit
+  // one cluster, a grid barrier over co-resident CTAs beyond that.
+  int mc = max_cluster_blocks(ns);
+  if (ntiles <= mc) {
     c->mode = SYNC_CLUSTER;
-    int mc = max_cluster_blocks(ns);
-    c->nblocks = std::max(1, std::min(mc, (n + TPB - 1) / TPB));
+    c->nblocks = std::max(1, ntiles);
   } else {
     c->mode = SYNC_GRID;
-    c->nblocks = std::max(1, std::min(maxco, std::max(ntiles, 148)));
+    c->nblocks = std::max(1, std::min(maxco, ntiles));
   }
   (void)ntiles;
 }
@@ -256,8 +258,8 @@ int xcal_hmesh_csr(xcal_hmesh m, int64_t *nnz, int32_t *rp, int32_t *col, int32_
   if (nnz) *nnz = P.nnz;
   if (rp) std::copy(P.row_ptr.begin(), P.row_ptr.end(), rp);
   if (col) std::copy(P.col.begin(), P.col.end(), col);
-  if (fl) std::copy(P.flev.begin(), P.flev.end(), fl);
-  if (bl) std::copy(P.blev.begin(), P.blev.end(), bl);
+  if (fl) std::copy(P.flev.begin(), P.flev.begin() + P.n, fl);
+  if (bl) std::copy(P.blev.begin(), P.blev.begin() + P.n, bl);
   if (nl) { nl[0] = P.nfl; nl[1] = P.nbl; }
   return XCAL_OK;
 }
@@ -284,7 +286,7 @@ int xcal_mesh_upload(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
   c->ns = (M.dim == 3) ? 3 : 2;
   KParams &h = c->hp;
   memset(&h, 0, sizeof(h));
-  h.n = P.n; h.nf = P.nf; h.nbf = P.nbf; h.dim = M.dim; h.ntiles = (P.n + TILE - 1) / TILE;
+  h.n = P.n; h.nf = P.nf; h.nbf = P.nbf; h.dim = M.dim; h.ntiles = P.np / TILE;
   std::vector<double> cx(P.n), cy(P.n), cz(P.n), fx(P.nf), fy(P.nf), fz(P.nf), nx(P.nf), ny(P.nf), nz(P.nf);
   for (int i = 0; i < P.n; ++i) { cx[i] = M.cc[3 * i]; cy[i] = M.cc[3 * i + 1]; cz[i] = M.cc[3 * i + 2]; }
   for (int f = 0; f < P.nf; ++f) {
@@ -297,18 +299,15 @@ int xcal_mesh_upload(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
   TRY(upload_c(c, B, h.wgt, M.fweight)); TRY(upload_c(c, B, h.fnx, nx)); TRY(upload_c(c, B, h.fny, ny));
   TRY(upload_c(c, B, h.fnz, nz)); TRY(upload_c(c, B, h.fcx, fx)); TRY(upload_c(c, B, h.fcy, fy));
   TRY(upload_c(c, B, h.fcz, fz)); TRY(upload_c(c, B, h.o1, P.o1)); TRY(upload_c(c, B, h.o2, P.o2));
-  TRY(upload_c(c, B, h.cf_ptr, P.cf_ptr)); TRY(upload_c(c, B, h.cf_face, P.cf_face));
-  TRY(upload_c(c, B, h.cf_nbr, P.cf_nbr)); TRY(upload_c(c, B, h.cf_slot, P.cf_slot));
-  TRY(upload_c(c, B, h.cf_sign, P.cf_sign)); TRY(upload_c(c, B, h.cf_first, P.cf_first));
+  TRY(upload_c(c, B, h.f_face, P.f_face)); TRY(upload_c(c, B, h.f_nbr, P.f_nbr));
+  TRY(upload_c(c, B, h.f_pos, P.f_pos)); TRY(upload_c(c, B, h.f_sign, P.f_sign));
+  TRY(upload_c(c, B, h.f_first, P.f_first));
   TRY(upload_c(c, B, h.cb_ptr, P.cb_ptr)); TRY(upload_c(c, B, h.cb_face, P.cb_face));
   TRY(upload_c(c, B, h.flev, P.flev)); TRY(upload_c(c, B, h.blev, P.blev));
-  TRY(upload_c(c, B, h.fl_ptr, P.fl_ptr)); TRY(upload_c(c, B, h.fl_rows, P.fl_rows));
-  TRY(upload_c(c, B, h.bl_ptr, P.bl_ptr)); TRY(upload_c(c, B, h.bl_rows, P.bl_rows));
-  h.nfl = P.nfl; h.nbl = P.nbl;
-  const int *rp, *col, *dg, *ts;
-  TRY(upload_c(c, B, rp, P.row_ptr)); TRY(upload_c(c, B, col, P.col));
-  TRY(upload_c(c, B, dg, P.diag)); TRY(upload_c(c, B, ts, P.tslot));
-  for (Mat *A : {&h.AU, &h.AP}) { A->rp = rp; A->col = col; A->diag = dg; A->tslot = ts; }
+  h.nfl = P.nfl; h.nbl = P.nbl; h.np = P.np; h.Wf = P.Wf;
+  const int *ecol, *etpos, *edpos;
+  TRY(upload_c(c, B, ecol, P.e_col)); TRY(upload_c(c, B, etpos, P.e_tpos)); TRY(upload_c(c, B, edpos, P.dpos));
+  for (Mat *A : {&h.AU, &h.AP}) { A->col = ecol; A->tpos = etpos; A->dpos = edpos; A->W = P.W; A->np = P.np; }
   choose_launch(c, P.n);
   c->have_mesh = true;
   return XCAL_OK;
@@ -342,8 +341,8 @@ int xcal_mesh_csr(xcal_ctx c, int64_t *nnz, int32_t *rp, int32_t *col, int32_t *
   if (nnz) *nnz = P.nnz;
   if (rp) std::copy(P.row_ptr.begin(), P.row_ptr.end(), rp);
   if (col) std::copy(P.col.begin(), P.col.end(), col);
-  if (fl) std::copy(P.flev.begin(), P.flev.end(), fl);
-  if (bl) std::copy(P.blev.begin(), P.blev.end(), bl);
+  if (fl) std::copy(P.flev.begin(), P.flev.begin() + P.n, fl);
+  if (bl) std::copy(P.blev.begin(), P.blev.begin() + P.n, bl);
   if (nl) { nl[0] = P.nfl; nl[1] = P.nbl; }
   return XCAL_OK;
 }
@@ -413,7 +412,8 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   c->run_cap = 0;
   KParams &h = c->hp;
   DevBuf &B = c->cbuf;
-  int n = c->prep.n, nf = c->prep.nf, nnz = c->prep.nnz, NS = c->ns;
+  int n = c->prep.n, nf = c->prep.nf, NS = c->ns;
+  size_t nnz = (size_t)c->prep.W * c->prep.np;
   TRY(build_bc(c, B, cfg->bc_U, cfg->nbc_U, h.bcU, c->tabU, true, "U"));
   TRY(build_bc(c, B, cfg->bc_p, cfg->nbc_p, h.bcP, c->tabP, false, "p"));
   h.div = cfg->schemes_U.divergence; h.time = cfg->schemes_U.time; h.grad = cfg->schemes_p.gradient;
@@ -430,8 +430,12 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   h.U = A((size_t)n * NS); h.Uz2 = A(n); h.p = A(n); h.gp = A((size_t)n * NS); h.bU = A((size_t)n * NS);
   h.bP = A(n); h.H = A((size_t)n * NS); h.rD = A(n); h.divH = A(n);
   h.mdot = A(nf); h.nueff = A(nf); h.rDf = A(nf); h.pf = A(nf); h.UfH = A((size_t)nf * NS);
-  for (KWork *w : {&h.wU}) { w->x = A((size_t)n * NS); w->r = A((size_t)n * NS); w->p = A((size_t)n * NS); w->v = A((size_t)n * NS); w->s = A((size_t)n * NS); w->t = A((size_t)n * NS); w->q = A((size_t)n * NS); }
-  { KWork *w = &h.wP; w->x = A(n); w->r = A(n); w->p = A(n); w->v = A(n); w->s = A(n); w->t = A(n); w->q = A(n); }
+  for (int k = 0; k < 2; ++k) {
+    KWork *w = (k == 0) ? &h.wU : &h.wP;
+    size_t m = (k == 0) ? (size_t)n * NS : (size_t)n;
+    w->x = A(m); w->s = A(m); w->t = A(m); w->q = A(m);
+    for (int b = 0; b < 2; ++b) { w->r[b] = A(m); w->p[b] = A(m); w->v[b] = A(m); }
+  }
   h.part = A((size_t)MAXK * h.ntiles);
   h.bar = B.alloc<Bar>(1);
   h.done = B.alloc<int>(1);
@@ -527,9 +531,8 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
   CUDA_TRY(c, cudaMemsetAsync(h.done, 0, sizeof(int), c->stream));
   h.mode = c->mode;
-  CUDA_TRY(c, cudaMemcpyAsync(c->dp, &h, sizeof(KParams), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-  if (iters > 0) CUDA_TRY(c, launch_program(c->ns, c->mode, c->nblocks, c->dp, prog, iters, c->stream));
+  if (iters > 0) CUDA_TRY(c, launch_program(c->ns, c->mode, c->nblocks, &h, prog, iters, c->stream));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   float ms = 0.f;
@@ -580,8 +583,15 @@ int xcal_equation_get(xcal_ctx c, int32_t which, double *vals, double *b0, doubl
   CUDA_TRY(c, cudaSetDevice(c->device));
   const KParams &h = c->hp;
   int n = c->prep.n, nnz = c->prep.nnz, NS = c->ns;
+  size_t ne = (size_t)c->prep.W * c->prep.np;
+  std::vector<double> ell(ne);
+  auto to_csr = [&](const double *dev) -> int {
+    CUDA_TRY(c, cudaMemcpy(ell.data(), dev, sizeof(double) * ne, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < nnz; ++k) vals[k] = ell[c->prep.csr2ell[k]];
+    return XCAL_OK;
+  };
   if (which == 0) {
-    if (vals) CUDA_TRY(c, cudaMemcpy(vals, h.AU.val, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+    if (vals) TRY(to_csr(h.AU.val));
     std::vector<double> b((size_t)n * NS);
     CUDA_TRY(c, cudaMemcpy(b.data(), h.bU, sizeof(double) * n * NS, cudaMemcpyDeviceToHost));
     double *dst[3] = {b0, b1, b2};
@@ -590,7 +600,7 @@ int xcal_equation_get(xcal_ctx c, int32_t which, double *vals, double *b0, doubl
     return XCAL_OK;
   }
   if (which == 1) {
-    if (vals) CUDA_TRY(c, cudaMemcpy(vals, h.AP.val, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+    if (vals) TRY(to_csr(h.AP.val));
     if (b0) CUDA_TRY(c, cudaMemcpy(b0, h.bP, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return XCAL_OK;
   }
@@ -634,32 +644,34 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   std::vector<int> fl(n, 0), bl(n, 0);
   for (int i = 0; i < n; ++i) { int l = 0; for (int k = rp[i]; k < dg[i]; ++k) l = std::max(l, fl[cl[k]] + 1); fl[i] = l; }
   for (int i = n - 1; i >= 0; --i) { int l = 0; for (int k = dg[i] + 1; k < rp[i + 1]; ++k) l = std::max(l, bl[cl[k]] + 1); bl[i] = l; }
-  auto bucket = [&](const std::vector<int> &lev, std::vector<int> &ptr, std::vector<int> &rows, int &nl) {
-    nl = 0;
-    for (int i = 0; i < n; ++i) nl = std::max(nl, lev[i] + 1);
-    ptr.assign(nl + 1, 0);
-    for (int i = 0; i < n; ++i) ptr[lev[i] + 1]++;
-    for (int l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
-    rows.resize(n);
-    std::vector<int> f(ptr.begin(), ptr.end() - 1);
-    for (int i = 0; i < n; ++i) rows[f[lev[i]]++] = i;
-  };
-  std::vector<int> flp, flr, blp, blr;
-  int nfl, nbl;
-  bucket(fl, flp, flr, nfl);
-  bucket(bl, blp, blr, nbl);
+  int nfl = 1, nbl = 1;
+  for (int i = 0; i < n; ++i) { nfl = std::max(nfl, fl[i] + 1); nbl = std::max(nbl, bl[i] + 1); }
+  int W = 0;
+  for (int i = 0; i < n; ++i) W = std::max(W, rp[i + 1] - rp[i]);
+  int np = ((n + TILE - 1) / TILE) * TILE;
+  std::vector<int> ecol((size_t)W * np, -1), etp((size_t)W * np, -1), edp(np, 0), c2e(nnz);
+  std::vector<double> ev((size_t)W * np, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      size_t e = (size_t)(k - rp[i]) * np + i;
+      ecol[e] = cl[k]; ev[e] = val[k]; c2e[k] = (int)e;
+    }
+  for (int i = 0; i < n; ++i) {
+    edp[i] = c2e[dg[i]];
+    for (int k = rp[i]; k < rp[i + 1]; ++k) etp[c2e[k]] = c2e[ts[k]];
+  }
+  fl.resize(np, 0);
+  bl.resize(np, 0);
   DevBuf B;
   KParams h;
   memset(&h, 0, sizeof(h));
-  h.n = n; h.ntiles = (n + TILE - 1) / TILE;
+  h.n = n; h.ntiles = np / TILE; h.np = np;
   TRY(upload_c(c, B, h.flev, fl)); TRY(upload_c(c, B, h.blev, bl));
-  TRY(upload_c(c, B, h.fl_ptr, flp)); TRY(upload_c(c, B, h.fl_rows, flr));
-  TRY(upload_c(c, B, h.bl_ptr, blp)); TRY(upload_c(c, B, h.bl_rows, blr));
   h.nfl = nfl; h.nbl = nbl;
-  TRY(upload_c(c, B, h.AU.rp, rp)); TRY(upload_c(c, B, h.AU.col, cl));
-  TRY(upload_c(c, B, h.AU.diag, dg)); TRY(upload_c(c, B, h.AU.tslot, ts));
-  std::vector<double> vv(val, val + nnz), bb(b, b + n), xx(x, x + n);
-  TRY(upload(c, B, h.AU.val, vv));
+  TRY(upload_c(c, B, h.AU.col, ecol)); TRY(upload_c(c, B, h.AU.tpos, etp)); TRY(upload_c(c, B, h.AU.dpos, edp));
+  h.AU.W = W; h.AU.np = np;
+  std::vector<double> bb(b, b + n), xx(x, x + n);
+  TRY(upload(c, B, h.AU.val, ev));
   TRY(upload(c, B, h.sb, bb));
   TRY(upload(c, B, h.U, xx));
   h.AU.precon = precon;
@@ -667,7 +679,8 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   auto A = [&](size_t cnt) { double *p = B.alloc<double>(cnt); if (!p) ok = false; return p; };
   h.AU.Dpiv = A(n); h.AU.Dinv = A(n);
   KWork &w = h.wU;
-  w.x = A(n); w.r = A(n); w.p = A(n); w.v = A(n); w.s = A(n); w.t = A(n); w.q = A(n);
+  w.x = A(n); w.s = A(n); w.t = A(n); w.q = A(n);
+  for (int k = 0; k < 2; ++k) { w.r[k] = A(n); w.p[k] = A(n); w.v[k] = A(n); }
   h.part = A((size_t)MAXK * h.ntiles);
   h.solve_out = A(2);
   h.bar = B.alloc<Bar>(1);
@@ -685,8 +698,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   }
   h.mode = mode;
   CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
-  CUDA_TRY(c, cudaMemcpyAsync(dp, &h, sizeof(KParams), cudaMemcpyHostToDevice, c->stream));
-  CUDA_TRY(c, launch_program(1, mode, nb, dp, PROG_SOLVE, 1, c->stream));
+  CUDA_TRY(c, launch_program(1, mode, nb, &h, PROG_SOLVE, 1, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   Bar bar;
   double so[2];

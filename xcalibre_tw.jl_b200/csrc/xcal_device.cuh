@@ -1,22 +1,29 @@
 // Device side of libxcal: data layout, barriers, canonical reductions and the
-// per-phase routines of one SIMPLE/PISO iteration.  Everything runs inside one
+// per-row routines of one SIMPLE/PISO iteration.  Everything runs inside one
 // persistent kernel (xcal_kernel.cu); phases are separated by a grid-wide
 // barrier (or a cluster / block barrier for small meshes).
 //
 // Arithmetic order: every floating-point expression reproduces the operation
 // order of the reference function it implements (cited per routine), and the
 // library is compiled with --fmad=false, so FP64 results equal the CPU oracle's
-// bit for bit.  Reductions follow the canonical fixed tree (tiles of 1024
-// values, 256 lanes x 4, warp shuffle-down tree, 8-way warp tree).
+// bit for bit.  Reductions follow the canonical fixed tree: tiles of 256 values
+// (one per lane), warp shuffle-down tree, 8-way warp tree; tile partials folded
+// per lane in ascending tile order, then the same tree.
+//
+// Layout: rows are padded to np = 256*ntiles.  The matrix is ELL: entry k of
+// row i at k*np + i (ascending columns, column -1 in unused entries), so a
+// warp's loads of one entry index are coalesced.  Per-cell internal-face lists
+// use the same layout (face -1 in unused entries).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace xcal {
 
-constexpr int TPB = 256;          // threads per CTA (fixed: canonical reduction lanes)
-constexpr int TILE = 1024;        // values per canonical reduction tile
-constexpr int MAXK = 8;           // partial-sum slots per phase
+constexpr int TPB = 256;          // threads per CTA = lanes of the canonical reduction
+constexpr int TILE = 256;         // rows per tile (one per thread)
+constexpr int MAXK = 8;           // partial-sum slots
+constexpr int WUNROLL = 8;        // matrix row width handled by the unrolled path
 enum { SYNC_BLOCK = 0, SYNC_CLUSTER = 1, SYNC_GRID = 2 };
 enum { PROG_SIMPLE = 0, PROG_PISO = 1, PROG_SOLVE = 2 };
 enum { ST_OK = 0, ST_TIMEOUT = 1 };
@@ -43,11 +50,14 @@ struct FieldBC {
   const int *fbc;       // [nbf] BC applied to each boundary face by correct_boundaries! (-1: none)
 };
 
+// Sparse matrix in ELL form (shared pattern, own values).
 struct Mat {
-  const int *rp, *col, *diag, *tslot;
-  double *val;
-  double *Dpiv, *Dinv;  // DILU pivots and their inverses (or diagonal scaling)
-  int precon;
+  const int *col;       // [W*np]
+  const int *tpos;      // [W*np] position of the transposed entry
+  const int *dpos;      // [np] position of the diagonal entry
+  double *val;          // [W*np]
+  double *Dpiv, *Dinv;  // DILU pivots and their inverses (or the diagonal scaling)
+  int precon, W, np;
 };
 
 struct KCfg {
@@ -55,28 +65,29 @@ struct KCfg {
   double atol, rtol;
 };
 
-// Krylov vectors, interleaved by system: v[i*NS + s]
+// Krylov vectors, interleaved by system: v[i*NS + s].  p, v and r have two
+// buffers each (the fused phases read the old values of neighbours while
+// writing new ones).
 struct KWork {
-  double *x, *r, *p, *v, *s, *t, *q;
+  double *x, *r[2], *p[2], *v[2], *s, *t, *q;
 };
 
 struct KParams {
-  int n, nf, nbf, dim, ntiles, mode;
+  int n, nf, nbf, dim, ntiles, np, mode, Wf;
   // geometry (read-only for the kernel's lifetime)
   const double *vol, *ccx, *ccy, *ccz;
   const double *area, *delta, *wgt, *fnx, *fny, *fnz, *fcx, *fcy, *fcz;
   const int *o1, *o2;
-  const int *cf_ptr, *cf_face, *cf_nbr, *cf_slot;
-  const signed char *cf_sign;
-  const unsigned char *cf_first;
+  const int *f_face, *f_nbr, *f_pos;      // [Wf*np]
+  const signed char *f_sign;
+  const unsigned char *f_first;
   const int *cb_ptr, *cb_face;
-  const int *flev, *blev;
+  const int *flev, *blev;                 // [np]
   int nfl, nbl;
-  const int *fl_ptr, *fl_rows, *bl_ptr, *bl_rows;
   Mat AU, AP;
   FieldBC bcU, bcP;
   // configuration
-  int div, time, grad, piso_corr;
+  int div, time, grad;
   double dt, nu, aU, aP;
   int has_pref, ref_cell;
   double pref;
@@ -84,7 +95,7 @@ struct KParams {
   // state
   double *U, *Uz2;      // U [n*NS] interleaved; Uz2: z component kept for 2D meshes
   double *p, *gp, *bU, *bP, *H, *rD, *divH;
-  double *mdot, *nueff, *rDf, *pf, *UfH;   // face fields (UfH [nf*NS])
+  double *mdot, *nueff, *rDf, *pf, *UfH;  // face fields (UfH [nf*NS])
   KWork wU, wP;
   double *part;         // [MAXK * ntiles]
   // outputs
@@ -93,10 +104,9 @@ struct KParams {
   int *done;            // iterations executed
   Bar *bar;
   // standalone solve
-  double *sb;           // right-hand side
-  int solve_solver;
+  double *sb;
+  int solve_solver, solve_itmax;
   double solve_atol, solve_rtol;
-  int solve_itmax;
   double *solve_out;    // [2]: iterations, final rNorm
 };
 
@@ -120,9 +130,7 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
   return v;
 }
 
-__device__ __forceinline__ int ld_volatile_i32(const int *p) {
-  return *(volatile const int *)p;
-}
+__device__ __forceinline__ int ld_volatile_i32(const int *p) { return *(volatile const int *)p; }
 
 constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;   // 2 s
 
@@ -146,19 +154,21 @@ struct Sync {
     epoch += 1;
     if (threadIdx.x == 0) {
       int good = 1;
-      unsigned long long target = epoch * (unsigned long long)nb;
+      const unsigned long long target = epoch * (unsigned long long)nb;
       __threadfence();
-      unsigned long long v = atomicAdd(&bar->count, 1ull) + 1ull;
+      const unsigned long long v = atomicAdd(&bar->count, 1ull) + 1ull;
       if (v < target) {
-        unsigned long long t0 = globaltimer();
+        const unsigned long long t0 = globaltimer();
         unsigned spins = 0;
         while (true) {
           if (ld_acquire_u64(&bar->count) >= target) break;
-          if (ld_volatile_i32(&bar->err)) { good = 0; break; }
-          if (((++spins) & 127u) == 0u && globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
-            atomicExch(&bar->err, ST_TIMEOUT);
-            good = 0;
-            break;
+          if (((++spins) & 63u) == 0u) {
+            if (ld_volatile_i32(&bar->err)) { good = 0; break; }
+            if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+              atomicExch(&bar->err, ST_TIMEOUT);
+              good = 0;
+              break;
+            }
           }
         }
       }
@@ -172,7 +182,7 @@ struct Sync {
 
 // ------------------------------------------------------ canonical reduction
 // Reduce K values held by each of the 256 threads with the fixed tree; the
-// result is returned in thread 0 (other threads get unspecified values).
+// result is valid in thread 0.
 template <int K>
 __device__ __forceinline__ void block_tree(double (&s)[K], double *sm /* [8*K] */) {
 #pragma unroll
@@ -196,16 +206,16 @@ __device__ __forceinline__ void block_tree(double (&s)[K], double *sm /* [8*K] *
   }
 }
 
-// Final sum of K partial arrays part[slot[k]*ntiles + t]; result broadcast to
-// every thread of the CTA through sm_out.
+// Final sum of K partial arrays part[k*ntiles + t]; the result is broadcast
+// to every thread of the CTA.
 template <int K>
-__device__ __forceinline__ void final_sum(const double *part, const int (&slot)[K], int ntiles,
-                                          double *sm, double *sm_out, double (&out)[K]) {
+__device__ __forceinline__ void final_sum(const double *part, int ntiles, double *sm, double *sm_out,
+                                          double (&out)[K]) {
   double s[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    const double *pp = part + (size_t)slot[k] * ntiles;
-    int t = threadIdx.x;
+    const double *pp = part + (size_t)k * ntiles;
+    const int t = threadIdx.x;
     double a = (t < ntiles) ? pp[t] : 0.0;
     for (int q = t + TPB; q < ntiles; q += TPB) a = a + pp[q];
     s[k] = a;
@@ -221,89 +231,112 @@ __device__ __forceinline__ void final_sum(const double *part, const int (&slot)[
 }
 
 // ------------------------------------------------------------- sparse rows
-// y_i = sum_k val[k]*x[col[k]] in ascending column order from 0.0: the order of
-// SparseArrays' CSC mul! (column scatter) as seen by one row.
-template <int NS>
-__device__ __forceinline__ void spmv_row(const Mat &A, const double *__restrict__ x, int i,
-                                         double (&y)[NS]) {
+// Row entries: all column indices of a row are loaded up front (independent,
+// coalesced); the sums then run in ascending column order.
+struct Row {
+  int c[WUNROLL];
+  int W;
+};
+__device__ __forceinline__ void load_row(const Mat &A, int i, Row &r) {
+  r.W = A.W;
+#pragma unroll
+  for (int k = 0; k < WUNROLL; ++k) r.c[k] = (k < A.W) ? __ldg(A.col + (size_t)k * A.np + i) : -1;
+}
+
+// y = sum_k val[k]*x[col[k]] in ascending column order from 0.0: the order of
+// SparseArrays' CSC mul! (column scatter) as seen by one row.  GetX(j, d)
+// returns component d of x at row j (it may compute the value on the fly).
+template <int NS, class GetX>
+__device__ __forceinline__ void spmv_row(const Mat &A, int i, GetX getx, double (&y)[NS]) {
 #pragma unroll
   for (int d = 0; d < NS; ++d) y[d] = 0.0;
-  const int b = __ldg(A.rp + i), e = __ldg(A.rp + i + 1);
-  for (int k = b; k < e; ++k) {
-    const double a = A.val[k];
-    const int j = __ldg(A.col + k);
+  if (A.W <= WUNROLL) {
+    Row r;
+    load_row(A, i, r);
 #pragma unroll
-    for (int d = 0; d < NS; ++d) y[d] = y[d] + a * x[(size_t)j * NS + d];
+    for (int k = 0; k < WUNROLL; ++k) {
+      if (r.c[k] >= 0) {
+        const double a = A.val[(size_t)k * A.np + i];
+#pragma unroll
+        for (int d = 0; d < NS; ++d) y[d] = y[d] + a * getx(r.c[k], d);
+      }
+    }
+  } else {
+    for (int k = 0; k < A.W; ++k) {
+      const int j = __ldg(A.col + (size_t)k * A.np + i);
+      if (j < 0) continue;
+      const double a = A.val[(size_t)k * A.np + i];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) y[d] = y[d] + a * getx(j, d);
+    }
   }
 }
 
 // DILU pivot of row i (update_dilu_diagonal!, preconditioners_1_DILU.jl:230-251):
 // D_i = A_ii - sum_{j<i} (A_ij*A_ji)/D_j over lower neighbours in ascending j.
 __device__ __forceinline__ void dilu_setup_row(const Mat &A, int i) {
-  const int dg = __ldg(A.diag + i);
-  double D = A.val[dg];
-  for (int k = __ldg(A.rp + i); k < dg; ++k) {
-    const int j = __ldg(A.col + k);
-    D = D - A.val[k] * A.val[__ldg(A.tslot + k)] / A.Dpiv[j];
+  double D = A.val[__ldg(A.dpos + i)];
+  for (int k = 0; k < A.W; ++k) {
+    const size_t e = (size_t)k * A.np + i;
+    const int j = __ldg(A.col + e);
+    if (j < 0 || j >= i) break;
+    D = D - A.val[e] * A.val[__ldg(A.tpos + e)] / A.Dpiv[j];
   }
   A.Dpiv[i] = D;
   A.Dinv[i] = 1 / D;
 }
 
 // Forward row (forward_substitution!, :253-279): o = in_i - sum_{j<i} (A_ij*out_j)*Dinv_j.
-// Rows without upper neighbours finish the backward step at once (x_i = c_i*Dinv_i).
-template <int NS>
-__device__ __forceinline__ void dilu_fwd_row(const Mat &A, const double *in, double *out, int i,
-                                             int blev_i, unsigned amask) {
-  const int dg = __ldg(A.diag + i), b = __ldg(A.rp + i);
-  double o[NS];
+// GetOut(j, d) returns out_j (possibly recomputed); rows without upper
+// neighbours also take the backward step at once (x_i = c_i*Dinv_i).
+template <int NS, class GetOut>
+__device__ __forceinline__ void dilu_fwd_row(const Mat &A, const double (&in)[NS], GetOut geto, int i,
+                                             int blev_i, double (&o)[NS]) {
 #pragma unroll
-  for (int d = 0; d < NS; ++d) o[d] = in[(size_t)i * NS + d];
-  for (int k = b; k < dg; ++k) {
-    const int j = __ldg(A.col + k);
-    const double a = A.val[k], dj = A.Dinv[j];
+  for (int d = 0; d < NS; ++d) o[d] = in[d];
+  for (int k = 0; k < A.W; ++k) {
+    const size_t e = (size_t)k * A.np + i;
+    const int j = __ldg(A.col + e);
+    if (j < 0 || j >= i) break;
+    const double a = A.val[e], dj = A.Dinv[j];
 #pragma unroll
-    for (int d = 0; d < NS; ++d) o[d] = o[d] - a * out[(size_t)j * NS + d] * dj;
+    for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * dj;
   }
   if (blev_i == 0) {
     const double di = A.Dinv[i];
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = o[d] * di;
   }
-#pragma unroll
-  for (int d = 0; d < NS; ++d)
-    if (amask & (1u << d)) out[(size_t)i * NS + d] = o[d];
 }
 
 // Backward row (backward_substitution!, :281-308): x_i = c_i*Dinv_i, then
 // x_i -= (A_ij*x_j)*Dinv_i for upper neighbours in ascending j.
 template <int NS>
-__device__ __forceinline__ void dilu_bwd_row(const Mat &A, double *out, int i, unsigned amask) {
-  const int dg = __ldg(A.diag + i), e = __ldg(A.rp + i + 1);
+__device__ __forceinline__ void dilu_bwd_row(const Mat &A, const double *out, int i, double (&o)[NS]) {
   const double di = A.Dinv[i];
-  double o[NS];
 #pragma unroll
   for (int d = 0; d < NS; ++d) o[d] = out[(size_t)i * NS + d] * di;
-  for (int k = dg + 1; k < e; ++k) {
-    const int j = __ldg(A.col + k);
-    const double a = A.val[k];
+  for (int k = 0; k < A.W; ++k) {
+    const size_t e = (size_t)k * A.np + i;
+    const int j = __ldg(A.col + e);
+    if (j <= i) continue;
+    const double a = A.val[e];
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = o[d] - a * out[(size_t)j * NS + d] * di;
   }
-#pragma unroll
-  for (int d = 0; d < NS; ++d)
-    if (amask & (1u << d)) out[(size_t)i * NS + d] = o[d];
 }
 
 // Diagonal preconditioners (Jacobi: 1/|A_ii|; NormDiagonal: 1/norm(column i)),
 // preconditioners_2_functions.jl:28-57.
 __device__ __forceinline__ void diag_precon_setup_row(const Mat &A, int i) {
   if (A.precon == 1) {
-    A.Dinv[i] = 1 / fabs(A.val[__ldg(A.diag + i)]);
+    A.Dinv[i] = 1 / fabs(A.val[__ldg(A.dpos + i)]);
   } else if (A.precon == 2) {
     double s = 0.0;
-    for (int k = __ldg(A.rp + i); k < __ldg(A.rp + i + 1); ++k) {
-      const double a = A.val[__ldg(A.tslot + k)];
+    for (int k = 0; k < A.W; ++k) {
+      const size_t e = (size_t)k * A.np + i;
+      if (__ldg(A.col + e) < 0) continue;
+      const double a = A.val[__ldg(A.tpos + e)];
       s += a * a;
     }
     A.Dinv[i] = 1 / sqrt(s);

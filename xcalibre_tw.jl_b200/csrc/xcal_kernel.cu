@@ -1,9 +1,9 @@
 // The persistent device program of libxcal: one launch runs `iters` SIMPLE (or
-// PISO) iterations, or one standalone Krylov solve.  Phases of an iteration are
-// separated by xcal::Sync barriers; see xcal_device.cuh for the arithmetic
-// contract.  Reference functions are cited at each phase.
-#include <cooperative_groups.h>
-
+// PISO) iterations, or one standalone Krylov solve.  Phases are separated by
+// xcal::Sync barriers; every phase is "tile owned" (tile t of 256 rows is always
+// processed by CTA t mod gridDim), so a CTA may reduce over its tiles at the end
+// of a phase sequence without another barrier.  Reference functions are cited at
+// each phase; xcal_device.cuh states the arithmetic contract.
 #include "xcal_device.cuh"
 #include "xcal_kernel.h"
 
@@ -26,36 +26,32 @@ struct Ctx {
   __device__ bool sync() { return S.sync(); }
 };
 
-// ---------------------------------------------------------------- loops
+// ---------------------------------------------------------------- phases
 template <class F>
 __device__ __forceinline__ void tile_each(const KParams &P, F f) {
-  for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x)
-#pragma unroll 1
-    for (int m = 0; m < 4; ++m) {
-      const int i = tile * TILE + m * TPB + threadIdx.x;
-      if (i < P.n) f(i);
-    }
+  for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+    const int i = t * TILE + threadIdx.x;
+    if (i < P.n) f(i);
+  }
 }
 
+// One row per thread per tile; with `reduce`, the K values returned by f are
+// summed per tile with the canonical tree into part[k*ntiles + t].
 template <int K, class F>
-__device__ __forceinline__ void tile_reduce(Ctx &C, const int (&slot)[K], F f) {
+__device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
   const KParams &P = *C.P;
-  for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
-    double acc[K];
-#pragma unroll 1
-    for (int m = 0; m < 4; ++m) {
-      const int i = tile * TILE + m * TPB + threadIdx.x;
-      double v[K];
+  for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+    const int i = t * TILE + threadIdx.x;
+    double v[K];
 #pragma unroll
-      for (int k = 0; k < K; ++k) v[k] = 0.0;
-      if (i < P.n) f(i, v);
+    for (int k = 0; k < K; ++k) v[k] = 0.0;
+    if (i < P.n) f(i, v);
+    if (reduce) {
+      block_tree<K>(v, C.sm);
+      if (threadIdx.x == 0)
 #pragma unroll
-      for (int k = 0; k < K; ++k) acc[k] = (m == 0) ? v[k] : acc[k] + v[k];
+        for (int k = 0; k < K; ++k) P.part[(size_t)k * P.ntiles + t] = v[k];
     }
-    block_tree<K>(acc, C.sm);
-    if (threadIdx.x == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) P.part[(size_t)slot[k] * P.ntiles + tile] = acc[k];
   }
 }
 
@@ -64,15 +60,26 @@ __device__ __forceinline__ void grid_each(int count, F f) {
   for (int i = blockIdx.x * TPB + threadIdx.x; i < count; i += gridDim.x * TPB) f(i);
 }
 
-// ------------------------------------------------------- preconditioning
-// Part of M^{-1} that needs no other row: DILU forward level 0 (and the
-// backward step of rows without upper neighbours), or a diagonal scaling.
 template <int NS>
-__device__ __forceinline__ void precon_fused_row(const KParams &P, const Mat &A, const double (&in)[NS],
-                                                 double *out, int i, unsigned amask) {
+__device__ __forceinline__ void ld(const double *a, int i, double (&o)[NS]) {
+#pragma unroll
+  for (int d = 0; d < NS; ++d) o[d] = a[(size_t)i * NS + d];
+}
+template <int NS>
+__device__ __forceinline__ void st(double *a, int i, const double (&o)[NS]) {
+#pragma unroll
+  for (int d = 0; d < NS; ++d) a[(size_t)i * NS + d] = o[d];
+}
+
+// ------------------------------------------------------- preconditioning
+// Row-local part of M^{-1}: DILU forward level 0 (and the backward step of
+// rows without upper neighbours) or a diagonal scaling.  Returns false when
+// the row has no row-local part (DILU rows of level >= 1).
+template <int NS>
+__device__ __forceinline__ bool precon_local(const KParams &P, const Mat &A, int i, const double (&in)[NS],
+                                             double (&o)[NS]) {
   if (A.precon == PRECON_DILU) {
-    if (__ldg(P.flev + i) != 0) return;
-    double o[NS];
+    if (__ldg(P.flev + i) != 0) return false;
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = in[d];
     if (__ldg(P.blev + i) == 0) {
@@ -80,120 +87,135 @@ __device__ __forceinline__ void precon_fused_row(const KParams &P, const Mat &A,
 #pragma unroll
       for (int d = 0; d < NS; ++d) o[d] = o[d] * di;
     }
+    return true;
+  }
+  const double di = A.Dinv[i];
 #pragma unroll
-    for (int d = 0; d < NS; ++d)
-      if (amask & (1u << d)) out[(size_t)i * NS + d] = o[d];
-  } else {
-    const double di = A.Dinv[i];
-#pragma unroll
-    for (int d = 0; d < NS; ++d)
-      if (amask & (1u << d)) out[(size_t)i * NS + d] = di * in[d];
-  }
-}
-
-// Remaining levels of M^{-1} (in -> out), after a phase that ran precon_fused_row.
-template <int NS>
-__device__ bool precon_levels(Ctx &C, const Mat &A, const double *in, double *out, unsigned amask) {
-  const KParams &P = *C.P;
-  if (A.precon != PRECON_DILU) return true;
-  for (int l = 1; l < P.nfl; ++l) {
-    const int b = __ldg(P.fl_ptr + l), e = __ldg(P.fl_ptr + l + 1);
-    grid_each(e - b, [&](int q) {
-      const int i = __ldg(P.fl_rows + b + q);
-      dilu_fwd_row<NS>(A, in, out, i, __ldg(P.blev + i), amask);
-    });
-    if (!C.sync()) return false;
-  }
-  for (int l = 1; l < P.nbl; ++l) {
-    const int b = __ldg(P.bl_ptr + l), e = __ldg(P.bl_ptr + l + 1);
-    grid_each(e - b, [&](int q) { dilu_bwd_row<NS>(A, out, __ldg(P.bl_rows + b + q), amask); });
-    if (!C.sync()) return false;
-  }
+  for (int d = 0; d < NS; ++d) o[d] = di * in[d];
   return true;
 }
 
-// update_preconditioner! for levels >= 1 fused with the first application
-// (level-0 rows were set up and applied in the assembly phase).
-template <int NS>
-__device__ bool precon_setup_apply(Ctx &C, const Mat &A, const double *in, double *out, unsigned amask) {
+// Number of phases of M^{-1} after its producer phase.  The producer did the
+// row-local part (and, with first_lvl == 2, forward level 1 as well).
+__device__ __forceinline__ int precon_tail_phases(const KParams &P, const Mat &A, bool setup, int first_lvl) {
+  if (A.precon != PRECON_DILU) return setup ? 1 : 0;
+  return max(0, P.nfl - first_lvl) + (P.nbl - 1);
+}
+
+// The remaining phases of M^{-1} (in -> out).  With `setup` the DILU pivots
+// (update_preconditioner!) are computed level by level in the same phases.
+// The last phase also computes the K partial sums red(i, v).
+template <int NS, int K, class Red>
+__device__ bool precon_tail(Ctx &C, const Mat &A, const double *in, double *out, bool setup, int first_lvl,
+                            Red red) {
   const KParams &P = *C.P;
+  const int nph = precon_tail_phases(P, A, setup, first_lvl);
+  if (nph == 0 && setup) {   // nothing left to apply: reduce in a phase of its own
+    tile_phase<K>(C, true, [&](int i, double (&v)[K]) { red(i, v); });
+    return C.sync();
+  }
   if (A.precon != PRECON_DILU) {
-    grid_each(P.n, [&](int i) {
+    if (!setup) return true;
+    tile_phase<K>(C, true, [&](int i, double (&v)[K]) {
       diag_precon_setup_row(A, i);
       const double di = A.Dinv[i];
 #pragma unroll
       for (int d = 0; d < NS; ++d) out[(size_t)i * NS + d] = di * in[(size_t)i * NS + d];
+      red(i, v);
     });
     return C.sync();
   }
-  for (int l = 1; l < P.nfl; ++l) {
-    const int b = __ldg(P.fl_ptr + l), e = __ldg(P.fl_ptr + l + 1);
-    grid_each(e - b, [&](int q) {
-      const int i = __ldg(P.fl_rows + b + q);
-      dilu_setup_row(A, i);
-      dilu_fwd_row<NS>(A, in, out, i, __ldg(P.blev + i), amask);
+  int ph = 0;
+  for (int l = first_lvl; l < P.nfl; ++l) {
+    const bool last = (++ph == nph);
+    tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
+      if (__ldg(P.flev + i) == l) {
+        if (setup) dilu_setup_row(A, i);
+        double iv[NS], o[NS];
+        ld<NS>(in, i, iv);
+        dilu_fwd_row<NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, __ldg(P.blev + i), o);
+        st<NS>(out, i, o);
+      }
+      if (last) red(i, v);
     });
     if (!C.sync()) return false;
   }
   for (int l = 1; l < P.nbl; ++l) {
-    const int b = __ldg(P.bl_ptr + l), e = __ldg(P.bl_ptr + l + 1);
-    grid_each(e - b, [&](int q) { dilu_bwd_row<NS>(A, out, __ldg(P.bl_rows + b + q), amask); });
+    const bool last = (++ph == nph);
+    tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
+      if (__ldg(P.blev + i) == l) {
+        double o[NS];
+        dilu_bwd_row<NS>(A, out, i, o);
+        st<NS>(out, i, o);
+      }
+      if (last) red(i, v);
+    });
     if (!C.sync()) return false;
   }
   return true;
 }
 
-// Krylov start for row i (Krylov.jl warm start): r0 = b - A*x0, x = 0, and the
-// row-local part of the first preconditioner application.  BiCGSTAB keeps r0
-// in q and preconditions into r; CG keeps r = r0 and preconditions into v.
+// Krylov start for row i (Krylov.jl warm start): r0 = b - A*x0 over the row
+// just assembled, x = 0, the DILU pivot of level-0 rows and the row-local part
+// of the first M^{-1}.  BiCGSTAB keeps r0 in q and preconditions into r[0];
+// CG keeps r[0] = r0 and preconditions into v[0].
 template <int NS>
 __device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A, const KWork &w,
-                                                const double (&b)[NS], const double *x0, int i,
-                                                int solver) {
+                                                const double (&b)[NS], const double *x0, int i, int solver) {
   double y[NS], r0[NS];
-  spmv_row<NS>(A, x0, i, y);
+  spmv_row<NS>(A, i, [&](int j, int d) { return x0[(size_t)j * NS + d]; }, y);
 #pragma unroll
   for (int d = 0; d < NS; ++d) {
     r0[d] = b[d] - y[d];
     w.x[(size_t)i * NS + d] = 0.0;
   }
   if (A.precon == PRECON_DILU && __ldg(P.flev + i) == 0) dilu_setup_row(A, i);
+  double o[NS];
+  const bool dilu = (A.precon == PRECON_DILU);
   if (solver == SOLVER_BICGSTAB) {
-#pragma unroll
-    for (int d = 0; d < NS; ++d) w.q[(size_t)i * NS + d] = r0[d];
-    if (A.precon == PRECON_DILU) precon_fused_row<NS>(P, A, r0, w.r, i, 0xffu);
+    st<NS>(w.q, i, r0);
+    if (dilu && precon_local<NS>(P, A, i, r0, o)) st<NS>(w.r[0], i, o);
   } else {
-#pragma unroll
-    for (int d = 0; d < NS; ++d) w.r[(size_t)i * NS + d] = r0[d];
-    if (A.precon == PRECON_DILU) precon_fused_row<NS>(P, A, r0, w.v, i, 0xffu);
+    st<NS>(w.r[0], i, r0);
+    if (dilu && precon_local<NS>(P, A, i, r0, o)) st<NS>(w.v[0], i, o);
   }
+}
+
+// Set-up phases of M and its first application after the assembly phase,
+// with the initial dot products (CG: <r,z>; BiCGSTAB: <b,r>, <r,r>).
+template <int NS>
+__device__ bool krylov_start(Ctx &C, const Mat &A, const KWork &w, const double *b, int solver) {
+  if (solver == SOLVER_BICGSTAB) {
+    return precon_tail<NS, 2 * NS>(C, A, w.q, w.r[0], true, 1, [&](int i, double (&v)[2 * NS]) {
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        const double rv = w.r[0][(size_t)i * NS + d];
+        v[2 * d] = b[(size_t)i * NS + d] * rv;
+        v[2 * d + 1] = rv * rv;
+      }
+    });
+  }
+  return precon_tail<NS, NS>(C, A, w.r[0], w.v[0], true, 1, [&](int i, double (&v)[NS]) {
+#pragma unroll
+    for (int d = 0; d < NS; ++d) v[d] = w.r[0][(size_t)i * NS + d] * w.v[0][(size_t)i * NS + d];
+  });
 }
 
 // ------------------------------------------------------------- BiCGSTAB
 // Krylov.jl 0.9.5 bicgstab! with left preconditioner M, N = I, c = b.
-// On entry r = M^{-1}(b - A x0), x = 0.  its[d] receives the iteration count.
+// Entry: r[0] = M^{-1}(b - A x0), x = 0, partials <b,r>, <r,r> in part.
+// Fused phases per iteration:
+//   A  p = r + beta*(p - omega*v) (recomputed for neighbours), q = A p, M^-1 level 0
+//   .. remaining M^-1 phases, last one reduces <b,v>
+//   D  s = r - alpha*v (recomputed for neighbours), x += alpha*p, q = A s, M^-1 level 0
+//   .. remaining M^-1 phases, last one reduces <t,s>, <t,t>
+//   G  x += omega*s, r = s - omega*t, reduces <b,r>, <r,r>
 template <int NS>
 __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb, const KCfg &cfg,
                          int (&its)[NS], double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   double red[2 * NS];
-  int slot2[2 * NS];
-#pragma unroll
-  for (int k = 0; k < 2 * NS; ++k) slot2[k] = k;
-  int slot1[NS];
-#pragma unroll
-  for (int k = 0; k < NS; ++k) slot1[k] = k;
-  tile_reduce<2 * NS>(C, slot2, [&](int i, double (&v)[2 * NS]) {
-#pragma unroll
-    for (int d = 0; d < NS; ++d) {
-      const double rv = w.r[(size_t)i * NS + d];
-      w.p[(size_t)i * NS + d] = rv;
-      v[2 * d] = bb[(size_t)i * NS + d] * rv;
-      v[2 * d + 1] = rv * rv;
-    }
-  });
-  if (!C.sync()) return false;
-  final_sum<2 * NS>(P.part, slot2, P.ntiles, C.sm, C.sm_out, red);
+  final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
   double rho[NS], alpha[NS], omega[NS], beta[NS], rnorm[NS], eps[NS], nrho[NS];
   unsigned active = 0;
 #pragma unroll
@@ -209,89 +231,105 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
     const bool solved = rnorm[d] <= eps[d], tired = 0 >= cfg.itmax;
     if (!(solved || tired)) active |= 1u << d;
   }
+  double *r = w.r[0];
+  const int tail = precon_tail_phases(P, A, false, 1);
+  int pc = 0;
+  bool first = true;
   while (active) {
 #pragma unroll
     for (int d = 0; d < NS; ++d)
       if (active & (1u << d)) { its[d] += 1; rho[d] = nrho[d]; }
-    // q = A y (y = p); v = M^{-1} q
-    tile_each(P, [&](int i) {
-      double y[NS];
-      spmv_row<NS>(A, w.p, i, y);
+    double *pn = w.p[pc], *po = w.p[pc ^ 1], *vn = w.v[pc], *vo = w.v[pc ^ 1];
+    auto getp = [&](int j, int d) -> double {
+      const size_t k = (size_t)j * NS + d;
+      if (first) return r[k];
+      const double pv = po[k] + (-omega[d]) * vo[k];
+      return r[k] + beta[d] * pv;
+    };
+    // A: p update, q = A p, M^{-1} row-local part
+    tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
+      double y[NS], pi[NS], o[NS];
+      spmv_row<NS>(A, i, getp, y);
+#pragma unroll
+      for (int d = 0; d < NS; ++d) pi[d] = getp(i, d);
 #pragma unroll
       for (int d = 0; d < NS; ++d)
-        if (active & (1u << d)) w.q[(size_t)i * NS + d] = y[d];
-      precon_fused_row<NS>(P, A, y, w.v, i, active);
-    });
-    if (!C.sync()) return false;
-    if (!precon_levels<NS>(C, A, w.q, w.v, active)) return false;
-    // alpha = rho / <c, v>
-    tile_reduce<NS>(C, slot1, [&](int i, double (&v)[NS]) {
+        if (active & (1u << d)) pn[(size_t)i * NS + d] = pi[d];
+      st<NS>(w.q, i, y);
+      if (precon_local<NS>(P, A, i, y, o)) st<NS>(vn, i, o);
+      if (tail == 0)
 #pragma unroll
-      for (int d = 0; d < NS; ++d) v[d] = bb[(size_t)i * NS + d] * w.v[(size_t)i * NS + d];
+        for (int d = 0; d < NS; ++d) v[d] = bb[(size_t)i * NS + d] * o[d];
     });
     if (!C.sync()) return false;
+    if (!precon_tail<NS, NS>(C, A, w.q, vn, false, 1, [&](int i, double (&v)[NS]) {
+#pragma unroll
+          for (int d = 0; d < NS; ++d) v[d] = bb[(size_t)i * NS + d] * vn[(size_t)i * NS + d];
+        }))
+      return false;
     {
       double cv[NS];
-      final_sum<NS>(P.part, slot1, P.ntiles, C.sm, C.sm_out, cv);
+      final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, cv);
 #pragma unroll
       for (int d = 0; d < NS; ++d)
         if (active & (1u << d)) alpha[d] = rho[d] / cv[d];
     }
-    // s = r - alpha*v ; x = x + alpha*y
-    tile_each(P, [&](int i) {
-#pragma unroll
-      for (int d = 0; d < NS; ++d)
-        if (active & (1u << d)) {
-          const size_t k = (size_t)i * NS + d;
-          w.s[k] = w.r[k] + (-alpha[d]) * w.v[k];
-          w.x[k] = w.x[k] + alpha[d] * w.p[k];
-        }
-    });
-    if (!C.sync()) return false;
-    // d = A z (z = s); t = M^{-1} d
-    tile_each(P, [&](int i) {
-      double y[NS];
-      spmv_row<NS>(A, w.s, i, y);
-#pragma unroll
-      for (int d = 0; d < NS; ++d)
-        if (active & (1u << d)) w.q[(size_t)i * NS + d] = y[d];
-      precon_fused_row<NS>(P, A, y, w.t, i, active);
-    });
-    if (!C.sync()) return false;
-    if (!precon_levels<NS>(C, A, w.q, w.t, active)) return false;
-    // omega = <t,s>/<t,t>
-    tile_reduce<2 * NS>(C, slot2, [&](int i, double (&v)[2 * NS]) {
+    auto gets = [&](int j, int d) -> double {
+      const size_t k = (size_t)j * NS + d;
+      return r[k] + (-alpha[d]) * vn[k];
+    };
+    // D: s, x += alpha p, q = A s, M^{-1} row-local part
+    tile_phase<2 * NS>(C, tail == 0, [&](int i, double (&v)[2 * NS]) {
+      double y[NS], o[NS], si[NS];
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
-        const double tv = w.t[k];
-        v[2 * d] = tv * w.s[k];
-        v[2 * d + 1] = tv * tv;
+        si[d] = gets(i, d);
+        if (active & (1u << d)) {
+          w.s[k] = si[d];
+          w.x[k] = w.x[k] + alpha[d] * pn[k];
+        }
       }
+      spmv_row<NS>(A, i, gets, y);
+      st<NS>(w.q, i, y);
+      if (precon_local<NS>(P, A, i, y, o)) st<NS>(w.t, i, o);
+      if (tail == 0)
+#pragma unroll
+        for (int d = 0; d < NS; ++d) { v[2 * d] = o[d] * si[d]; v[2 * d + 1] = o[d] * o[d]; }
     });
     if (!C.sync()) return false;
-    final_sum<2 * NS>(P.part, slot2, P.ntiles, C.sm, C.sm_out, red);
+    if (!precon_tail<NS, 2 * NS>(C, A, w.q, w.t, false, 1, [&](int i, double (&v)[2 * NS]) {
+#pragma unroll
+          for (int d = 0; d < NS; ++d) {
+            const size_t k = (size_t)i * NS + d;
+            const double tv = w.t[k];
+            v[2 * d] = tv * w.s[k];
+            v[2 * d + 1] = tv * tv;
+          }
+        }))
+      return false;
+    final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
 #pragma unroll
     for (int d = 0; d < NS; ++d)
       if (active & (1u << d)) omega[d] = red[2 * d] / red[2 * d + 1];
-    // x = x + omega*z ; r = s - omega*t ; <c,r>, <r,r>
-    tile_reduce<2 * NS>(C, slot2, [&](int i, double (&v)[2 * NS]) {
+    // G: x += omega s, r = s - omega t, <b,r>, <r,r>
+    tile_phase<2 * NS>(C, true, [&](int i, double (&v)[2 * NS]) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
-        double rv = w.r[k];
+        double rv = r[k];
         if (active & (1u << d)) {
           const double sv = w.s[k];
           w.x[k] = w.x[k] + omega[d] * sv;
           rv = sv + (-omega[d]) * w.t[k];
-          w.r[k] = rv;
+          r[k] = rv;
         }
         v[2 * d] = bb[k] * rv;
         v[2 * d + 1] = rv * rv;
       }
     });
     if (!C.sync()) return false;
-    final_sum<2 * NS>(P.part, slot2, P.ntiles, C.sm, C.sm_out, red);
+    final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
     unsigned cont = 0;
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
@@ -305,20 +343,9 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
       const bool breakdown = (alpha[d] == 0.0 || isnan(alpha[d]));
       if (!(solved || tired || breakdown)) cont |= 1u << d;
     }
-    if (cont) {
-      // p = p - omega*v ; p = r + beta*p
-      tile_each(P, [&](int i) {
-#pragma unroll
-        for (int d = 0; d < NS; ++d)
-          if (cont & (1u << d)) {
-            const size_t k = (size_t)i * NS + d;
-            double pv = w.p[k] + (-omega[d]) * w.v[k];
-            w.p[k] = w.r[k] + beta[d] * pv;
-          }
-      });
-      if (!C.sync()) return false;
-    }
     active = cont;
+    first = false;
+    pc ^= 1;
   }
 #pragma unroll
   for (int d = 0; d < NS; ++d) rnorm_out[d] = rnorm[d];
@@ -329,27 +356,19 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
 // Krylov.jl 0.9.5 cg! with preconditioner M.  The sign of <r,z> at the start
 // selects the formulation: for a negative definite system CG runs on (-A)x=-b,
 // i.e. <r,z> and <p,Ap> enter with their sign flipped (negation is exact).
-// On entry r = b - A x0, v = M^{-1} r, x = 0.
+// Entry: r[0] = b - A x0, v[0] = M^{-1} r, x = 0, partial <r,z> in part.
+// Fused phases per iteration:
+//   A  p = z + beta*p (recomputed for neighbours), q = A p, reduces <p,q>
+//   B  x += alpha p, r -= alpha q, M^-1 levels 0 and 1 (level-0 values of
+//      neighbours recomputed), backward step of rows without upper neighbours
+//   .. remaining M^-1 phases, the last reduces <r,z>
 template <int NS>
 __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&its)[NS],
                    double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   const double EPS = 2.220446049250313e-16;
-  int slot1[NS];
-#pragma unroll
-  for (int k = 0; k < NS; ++k) slot1[k] = k;
   double red[NS];
-  tile_reduce<NS>(C, slot1, [&](int i, double (&v)[NS]) {
-#pragma unroll
-    for (int d = 0; d < NS; ++d) {
-      const size_t k = (size_t)i * NS + d;
-      const double z = w.v[k];
-      w.p[k] = z;
-      v[d] = w.r[k] * z;
-    }
-  });
-  if (!C.sync()) return false;
-  final_sum<NS>(P.part, slot1, P.ntiles, C.sm, C.sm_out, red);
+  final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
   double gamma[NS], sgn[NS], rnorm[NS], pn2[NS], eps[NS], alpha[NS], beta[NS];
   unsigned active = 0;
 #pragma unroll
@@ -364,22 +383,34 @@ __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&
     const bool solved = rnorm[d] <= eps[d], tired = 0 >= cfg.itmax;
     if (!(solved || tired)) active |= 1u << d;
   }
+  const double *z = w.v[0];
+  double *zw = w.v[0];
+  const bool dilu = (A.precon == PRECON_DILU);
+  const bool lvl1 = dilu && P.nfl >= 2;
+  const int tail = dilu ? precon_tail_phases(P, A, false, 2) : 0;
+  int rc = 0, pc = 0;
+  bool first = true;
   while (active) {
-    // Ap
-    tile_each(P, [&](int i) {
+    double *pn = w.p[pc], *po = w.p[pc ^ 1];
+    auto getp = [&](int j, int d) -> double {
+      const size_t k = (size_t)j * NS + d;
+      if (first) return z[k];
+      return z[k] + beta[d] * po[k];
+    };
+    // A: p update, q = A p, <p,q>
+    tile_phase<NS>(C, true, [&](int i, double (&v)[NS]) {
       double y[NS];
-      spmv_row<NS>(A, w.p, i, y);
+      spmv_row<NS>(A, i, getp, y);
 #pragma unroll
-      for (int d = 0; d < NS; ++d)
-        if (active & (1u << d)) w.q[(size_t)i * NS + d] = y[d];
+      for (int d = 0; d < NS; ++d) {
+        const double pi = getp(i, d);
+        if (active & (1u << d)) pn[(size_t)i * NS + d] = pi;
+        v[d] = pi * y[d];
+      }
+      st<NS>(w.q, i, y);
     });
     if (!C.sync()) return false;
-    tile_reduce<NS>(C, slot1, [&](int i, double (&v)[NS]) {
-#pragma unroll
-      for (int d = 0; d < NS; ++d) v[d] = w.p[(size_t)i * NS + d] * w.q[(size_t)i * NS + d];
-    });
-    if (!C.sync()) return false;
-    final_sum<NS>(P.part, slot1, P.ntiles, C.sm, C.sm_out, red);
+    final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
     unsigned upd = 0;
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
@@ -391,29 +422,40 @@ __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&
     }
     active = upd;
     if (!active) break;
-    // x += alpha p ; r -= alpha Ap ; z = M^{-1} r (row-local part)
-    tile_each(P, [&](int i) {
-      double rr[NS];
+    double *ro = w.r[rc], *rn = w.r[rc ^ 1];
+    auto getr = [&](int j, int d) -> double {
+      const size_t k = (size_t)j * NS + d;
+      return ro[k] + (-alpha[d]) * w.q[k];
+    };
+    // B: x, r updates and M^{-1} levels 0/1
+    tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
+      double rr[NS], o[NS];
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
-        rr[d] = w.r[k];
+        rr[d] = getr(i, d);
         if (active & (1u << d)) {
-          w.x[k] = w.x[k] + alpha[d] * w.p[k];
-          rr[d] = rr[d] + (-alpha[d]) * w.q[k];
-          w.r[k] = rr[d];
+          w.x[k] = w.x[k] + alpha[d] * pn[k];
+          rn[k] = rr[d];
         }
       }
-      precon_fused_row<NS>(P, A, rr, w.v, i, active);
-    });
-    if (!C.sync()) return false;
-    if (!precon_levels<NS>(C, A, w.r, w.v, active)) return false;
-    tile_reduce<NS>(C, slot1, [&](int i, double (&v)[NS]) {
+      bool have = precon_local<NS>(P, A, i, rr, o);
+      if (!have && lvl1 && __ldg(P.flev + i) == 1) {
+        dilu_fwd_row<NS>(A, rr, getr, i, __ldg(P.blev + i), o);
+        have = true;
+      }
+      if (have) st<NS>(zw, i, o);
+      if (tail == 0)
 #pragma unroll
-      for (int d = 0; d < NS; ++d) v[d] = w.r[(size_t)i * NS + d] * w.v[(size_t)i * NS + d];
+        for (int d = 0; d < NS; ++d) v[d] = rr[d] * o[d];
     });
     if (!C.sync()) return false;
-    final_sum<NS>(P.part, slot1, P.ntiles, C.sm, C.sm_out, red);
+    if (dilu && !precon_tail<NS, NS>(C, A, rn, zw, false, 2, [&](int i, double (&v)[NS]) {
+#pragma unroll
+          for (int d = 0; d < NS; ++d) v[d] = rn[(size_t)i * NS + d] * z[(size_t)i * NS + d];
+        }))
+      return false;
+    final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
     unsigned cont = 0;
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
@@ -431,18 +473,10 @@ __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&
       const bool tired = its[d] >= cfg.itmax;
       if (!(solved || tired)) cont |= 1u << d;
     }
-    if (cont) {
-      tile_each(P, [&](int i) {
-#pragma unroll
-        for (int d = 0; d < NS; ++d)
-          if (cont & (1u << d)) {
-            const size_t k = (size_t)i * NS + d;
-            w.p[k] = w.v[k] + beta[d] * w.p[k];
-          }
-      });
-      if (!C.sync()) return false;
-    }
     active = cont;
+    first = false;
+    rc ^= 1;
+    pc ^= 1;
   }
 #pragma unroll
   for (int d = 0; d < NS; ++d) rnorm_out[d] = rnorm[d];
@@ -468,11 +502,12 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
   const Mat &A = P.AU;
   const double vol = __ldg(P.vol + i);
   double acc = 0.0;
-  const int cb = __ldg(P.cf_ptr + i), ce = __ldg(P.cf_ptr + i + 1);
-  for (int k = cb; k < ce; ++k) {
-    const int f = __ldg(P.cf_face + k);
-    const double ns = (double)__ldg(P.cf_sign + k);
-    const int slot = __ldg(P.cf_slot + k);
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    const double ns = (double)__ldg(P.f_sign + e);
+    const int pos = __ldg(P.f_pos + e);
     double t2;
     const double mf = P.mdot[f];
     if (P.div == DIV_UPWIND) {
@@ -480,12 +515,11 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
       acc += jmax(ap, 0.0);
       t2 = -jmax(-ap, 0.0);
     } else {
-      const int nb = __ldg(P.cf_nbr + k);
-      const double xfx = __ldg(P.fcx + f), xfy = __ldg(P.fcy + f), xfz = __ldg(P.fcz + f);
-      const double xcx = __ldg(P.ccx + i), xcy = __ldg(P.ccy + i), xcz = __ldg(P.ccz + i);
-      const double xnx = __ldg(P.ccx + nb), xny = __ldg(P.ccy + nb), xnz = __ldg(P.ccz + nb);
-      const double ax = xfx - xcx, ay = xfy - xcy, az = xfz - xcz;
-      const double bx = xnx - xcx, by = xny - xcy, bz = xnz - xcz;
+      const int nb = __ldg(P.f_nbr + e);
+      const double ax = __ldg(P.fcx + f) - __ldg(P.ccx + i), ay = __ldg(P.fcy + f) - __ldg(P.ccy + i),
+                   az = __ldg(P.fcz + f) - __ldg(P.ccz + i);
+      const double bx = __ldg(P.ccx + nb) - __ldg(P.ccx + i), by = __ldg(P.ccy + nb) - __ldg(P.ccy + i),
+                   bz = __ldg(P.ccz + nb) - __ldg(P.ccz + i);
       const double weight = sqrt((ax * ax + ay * ay) + az * az) / sqrt((bx * bx + by * by) + bz * bz);
       const double omw = 1.0 - weight;
       const double ap = 1.0 * (mf * ns);
@@ -495,8 +529,8 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
     const double ap3 = -1.0 * ((-P.nueff[f]) * __ldg(P.area + f)) / __ldg(P.delta + f);
     acc += ap3;
     const double t3 = -ap3;
-    const double base = __ldg(P.cf_first + k) ? 0.0 : A.val[slot];
-    A.val[slot] = (base + t2) + t3;
+    const double base = __ldg(P.f_first + e) ? 0.0 : A.val[pos];
+    A.val[pos] = (base + t2) + t3;
   }
   double prev[NS];
 #pragma unroll
@@ -542,10 +576,18 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
 #pragma unroll
     for (int d = 0; d < NS; ++d) b[d] += (1.0 - P.aU) * acc * prev[d];
   }
-  A.val[__ldg(A.diag + i)] = acc;
+  A.val[__ldg(A.dpos + i)] = acc;
   P.rD[i] = vol / acc;
-#pragma unroll
-  for (int d = 0; d < NS; ++d) P.bU[(size_t)i * NS + d] = b[d];
+  st<NS>(P.bU, i, b);
+}
+
+// u . S_f of a face vector field (flux!/div!: psif[fID] . (area*normal))
+template <int NS>
+__device__ __forceinline__ double face_dot_S(const KParams &P, const double *uf, int f) {
+  const double a = __ldg(P.area + f);
+  double s = uf[(size_t)f * NS] * (a * __ldg(P.fnx + f)) + uf[(size_t)f * NS + 1] * (a * __ldg(P.fny + f));
+  if (NS == 3) s = s + uf[(size_t)f * NS + 2] * (a * __ldg(P.fnz + f));
+  return s;
 }
 
 // Pressure row: div!(divHv, Uf) (Calculate_0_divergence.jl:75-107) then
@@ -555,31 +597,26 @@ template <int NS>
 __device__ __forceinline__ double pressure_row(const KParams &P, int i) {
   const Mat &A = P.AP;
   const double vol = __ldg(P.vol + i);
-  const int cb = __ldg(P.cf_ptr + i), ce = __ldg(P.cf_ptr + i + 1);
   double dv = 0.0;
-  for (int k = cb; k < ce; ++k) {
-    const int f = __ldg(P.cf_face + k);
-    const double a = __ldg(P.area + f);
-    double s = P.UfH[(size_t)f * NS] * (a * __ldg(P.fnx + f)) + P.UfH[(size_t)f * NS + 1] * (a * __ldg(P.fny + f));
-    if (NS == 3) s = s + P.UfH[(size_t)f * NS + 2] * (a * __ldg(P.fnz + f));
-    dv += s * (double)__ldg(P.cf_sign + k) / vol;
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    dv += face_dot_S<NS>(P, P.UfH, f) * (double)__ldg(P.f_sign + e) / vol;
   }
-  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q) {
-    const int f = __ldg(P.cb_face + q);
-    const double a = __ldg(P.area + f);
-    double s = P.UfH[(size_t)f * NS] * (a * __ldg(P.fnx + f)) + P.UfH[(size_t)f * NS + 1] * (a * __ldg(P.fny + f));
-    if (NS == 3) s = s + P.UfH[(size_t)f * NS + 2] * (a * __ldg(P.fnz + f));
-    dv += s / vol;
-  }
+  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q)
+    dv += face_dot_S<NS>(P, P.UfH, __ldg(P.cb_face + q)) / vol;
   P.divH[i] = dv;
   double acc = 0.0;
-  for (int k = cb; k < ce; ++k) {
-    const int f = __ldg(P.cf_face + k);
-    const int slot = __ldg(P.cf_slot + k);
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    const int pos = __ldg(P.f_pos + e);
     const double ap = 1.0 * ((-P.rDf[f]) * __ldg(P.area + f)) / __ldg(P.delta + f);
     acc += ap;
-    const double base = __ldg(P.cf_first + k) ? 0.0 : A.val[slot];
-    A.val[slot] = base + (-ap);
+    const double base = __ldg(P.f_first + e) ? 0.0 : A.val[pos];
+    A.val[pos] = base + (-ap);
   }
   double b = 0.0;
   b += 1.0 * dv * vol;
@@ -598,17 +635,38 @@ __device__ __forceinline__ double pressure_row(const KParams &P, int i) {
     b += acc * P.pref;
     acc += acc;
   }
-  A.val[__ldg(A.diag + i)] = acc;
+  A.val[__ldg(A.dpos + i)] = acc;
   P.bP[i] = b;
   return b;
 }
 
+// H! sums (Solvers_0_functions.jl:110-140): H = (b - sum_n A_cn U_n) * (1/A_cc),
+// ux's matrix for every component, neighbours in face order.
+template <int NS>
+__device__ __forceinline__ void H_row(const KParams &P, int i, const double (&bb)[NS]) {
+  const Mat &A = P.AU;
+  double sum[NS];
+#pragma unroll
+  for (int d = 0; d < NS; ++d) sum[d] = 0.0;
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    const int nb = __ldg(P.f_nbr + e);
+    const double a = A.val[__ldg(P.f_pos + e)];
+#pragma unroll
+    for (int d = 0; d < NS; ++d) sum[d] += a * P.U[(size_t)nb * NS + d];
+  }
+  const double rDc = 1 / A.val[__ldg(A.dpos + i)];
+#pragma unroll
+  for (int d = 0; d < NS; ++d) P.H[(size_t)i * NS + d] = (bb[d] - sum[d]) * rDc;
+}
+
 // ------------------------------------------------------------ face fields
 // interpolate! (Calculate_2_interpolation.jl:241-277) plus correct_boundaries!
-// (:135-237) for a vector cell field; returns the face value in u[].
+// (:135-237) for a vector cell field.
 template <int NS>
-__device__ __forceinline__ void face_vector(const KParams &P, const double *cellv, int f,
-                                            double (&u)[NS]) {
+__device__ __forceinline__ void face_vector(const KParams &P, const double *cellv, int f, double (&u)[NS]) {
   const double w = __ldg(P.wgt + f);
   const double omw = 1.0 - w;
   const int a = __ldg(P.o1 + f), b = __ldg(P.o2 + f);
@@ -624,8 +682,8 @@ __device__ __forceinline__ void face_vector(const KParams &P, const double *cell
   }
 }
 
-__device__ __forceinline__ double face_scalar(const KParams &P, const double *cellv, int f,
-                                              const FieldBC &bc, bool midpoint) {
+__device__ __forceinline__ double face_scalar(const KParams &P, const double *cellv, int f, const FieldBC &bc,
+                                              bool midpoint) {
   const int a = __ldg(P.o1 + f), b = __ldg(P.o2 + f);
   double v;
   if (midpoint) {
@@ -660,9 +718,11 @@ __device__ __forceinline__ void face_mdot(const KParams &P, int f) {
 template <int NS>
 __device__ __forceinline__ void green_gauss_row(const KParams &P, const double *pf, int i, double (&g)[NS]) {
   double r[3] = {0.0, 0.0, 0.0};
-  for (int k = __ldg(P.cf_ptr + i); k < __ldg(P.cf_ptr + i + 1); ++k) {
-    const int f = __ldg(P.cf_face + k);
-    const double ns = (double)__ldg(P.cf_sign + k);
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    const double ns = (double)__ldg(P.f_sign + e);
     const double a = __ldg(P.area + f), v = pf[f];
     r[0] += v * ((a * __ldg(P.fnx + f)) * ns);
     r[1] += v * ((a * __ldg(P.fny + f)) * ns);
@@ -675,9 +735,15 @@ __device__ __forceinline__ void green_gauss_row(const KParams &P, const double *
     const int f = __ldg(P.cb_face + q);
     const double a = __ldg(P.area + f), v = pf[f];
     double bx = v * (a * __ldg(P.fnx + f)), by = v * (a * __ldg(P.fny + f));
-    bx /= vol; by /= vol;
-    r[0] += bx; r[1] += by;
-    if (NS == 3) { double bz = v * (a * __ldg(P.fnz + f)); bz /= vol; r[2] += bz; }
+    bx /= vol;
+    by /= vol;
+    r[0] += bx;
+    r[1] += by;
+    if (NS == 3) {
+      double bz = v * (a * __ldg(P.fnz + f));
+      bz /= vol;
+      r[2] += bz;
+    }
   }
 #pragma unroll
   for (int d = 0; d < NS; ++d) g[d] = r[d];
@@ -714,8 +780,7 @@ __device__ bool gradient_p(Ctx &C, bool correct_u) {
     tile_each(P, [&](int i) {
       double g[NS];
       green_gauss_row<NS>(P, P.pf, i, g);
-#pragma unroll
-      for (int d = 0; d < NS; ++d) P.gp[(size_t)i * NS + d] = g[d];
+      st<NS>(P.gp, i, g);
       if (last && correct_u) {
         const double rdi = P.rD[i];
 #pragma unroll
@@ -759,14 +824,11 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       krylov_init_row<NS>(P, P.AU, P.wU, b, P.U, i, P.kU.solver);
     });
     if (!C.sync()) return;
-    {
-      const double *in = (P.kU.solver == SOLVER_BICGSTAB) ? P.wU.q : P.wU.r;
-      double *out = (P.kU.solver == SOLVER_BICGSTAB) ? P.wU.r : P.wU.v;
-      if (!precon_setup_apply<NS>(C, P.AU, in, out, 0xffu)) return;
-    }
+    if (!krylov_start<NS>(C, P.AU, P.wU, P.bU, P.kU.solver)) return;
     int itsU[NS];
     double rnU[NS];
     if (!krylov<NS>(C, P.AU, P.wU, P.bU, P.kU, P.kU.solver, itsU, rnU)) return;
+    // run! copy-back: U = x + x0
     tile_each(P, [&](int i) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
@@ -776,40 +838,25 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     });
     if (!C.sync()) return;
     // ---- residual!(R_ux..), remove_pressure_source!, H!
+    tile_phase<2 * NS>(C, true, [&](int i, double (&v)[2 * NS]) {
+      double y[NS], bb[NS];
+      spmv_row<NS>(P.AU, i, [&](int j, int d) { return P.U[(size_t)j * NS + d]; }, y);
+      const double vol = __ldg(P.vol + i);
+      ld<NS>(P.bU, i, bb);
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        const double df = y[d] - bb[d];
+        v[2 * d] = df * df;
+        v[2 * d + 1] = bb[d] * bb[d];
+        bb[d] -= -1.0 * P.gp[(size_t)i * NS + d] * vol;
+      }
+      st<NS>(P.bU, i, bb);
+      H_row<NS>(P, i, bb);
+    });
+    if (!C.sync()) return;
     {
-      int slot[2 * NS];
-#pragma unroll
-      for (int k = 0; k < 2 * NS; ++k) slot[k] = k;
-      tile_reduce<2 * NS>(C, slot, [&](int i, double (&v)[2 * NS]) {
-        const Mat &A = P.AU;
-        double y[NS];
-        spmv_row<NS>(A, P.U, i, y);
-        const double vol = __ldg(P.vol + i);
-        double bb[NS], sum[NS];
-#pragma unroll
-        for (int d = 0; d < NS; ++d) {
-          bb[d] = P.bU[(size_t)i * NS + d];
-          const double df = y[d] - bb[d];
-          v[2 * d] = df * df;
-          v[2 * d + 1] = bb[d] * bb[d];
-          bb[d] -= -1.0 * P.gp[(size_t)i * NS + d] * vol;
-          P.bU[(size_t)i * NS + d] = bb[d];
-          sum[d] = 0.0;
-        }
-        for (int k = __ldg(P.cf_ptr + i); k < __ldg(P.cf_ptr + i + 1); ++k) {
-          const int nb = __ldg(P.cf_nbr + k);
-          const double a = A.val[__ldg(P.cf_slot + k)];
-#pragma unroll
-          for (int d = 0; d < NS; ++d) sum[d] += a * P.U[(size_t)nb * NS + d];
-        }
-        const double Dd = A.val[__ldg(A.diag + i)];
-        const double rDc = 1 / Dd;
-#pragma unroll
-        for (int d = 0; d < NS; ++d) P.H[(size_t)i * NS + d] = (bb[d] - sum[d]) * rDc;
-      });
-      if (!C.sync()) return;
       double red[2 * NS];
-      final_sum<2 * NS>(P.part, slot, P.ntiles, C.sm, C.sm_out, red);
+      final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
 #pragma unroll
       for (int d = 0; d < NS; ++d) Rit[d] = sqrt(red[2 * d] / (double)P.n) / sqrt(red[2 * d + 1]);
       if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -824,19 +871,9 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     for (int corr = 0; corr < ncorr; ++corr) {
       if (corr > 0) {   // H! again with the corrected U (PISO corrector loop)
         tile_each(P, [&](int i) {
-          const Mat &A = P.AU;
-          double sum[NS];
-#pragma unroll
-          for (int d = 0; d < NS; ++d) sum[d] = 0.0;
-          for (int k = __ldg(P.cf_ptr + i); k < __ldg(P.cf_ptr + i + 1); ++k) {
-            const int nb = __ldg(P.cf_nbr + k);
-            const double a = A.val[__ldg(P.cf_slot + k)];
-#pragma unroll
-            for (int d = 0; d < NS; ++d) sum[d] += a * P.U[(size_t)nb * NS + d];
-          }
-          const double rDc = 1 / A.val[__ldg(A.diag + i)];
-#pragma unroll
-          for (int d = 0; d < NS; ++d) P.H[(size_t)i * NS + d] = (P.bU[(size_t)i * NS + d] - sum[d]) * rDc;
+          double bb[NS];
+          ld<NS>(P.bU, i, bb);
+          H_row<NS>(P, i, bb);
         });
         if (!C.sync()) return;
       }
@@ -858,11 +895,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
         krylov_init_row<1>(P, P.AP, P.wP, b, P.p, i, P.kP.solver);
       });
       if (!C.sync()) return;
-      {
-        const double *in = (P.kP.solver == SOLVER_BICGSTAB) ? P.wP.q : P.wP.r;
-        double *out = (P.kP.solver == SOLVER_BICGSTAB) ? P.wP.r : P.wP.v;
-        if (!precon_setup_apply<1>(C, P.AP, in, out, 0xffu)) return;
-      }
+      if (!krylov_start<1>(C, P.AP, P.wP, P.bP, P.kP.solver)) return;
       int itsP[1];
       double rnP[1];
       if (!krylov<1>(C, P.AP, P.wP, P.bP, P.kP, P.kP.solver, itsP, rnP)) return;
@@ -874,20 +907,19 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       });
       if (!C.sync()) return;
       // residual!(R_p) and the face interpolation of grad!(grad p)
+      tile_phase<2>(C, true, [&](int i, double (&v)[2]) {
+        double y[1];
+        spmv_row<1>(P.AP, i, [&](int j, int d) { return P.p[j]; }, y);
+        const double bb = P.bP[i];
+        const double df = y[0] - bb;
+        v[0] = df * df;
+        v[1] = bb * bb;
+      });
+      grid_each(P.nf, [&](int f) { P.pf[f] = face_scalar(P, P.p, f, P.bcP, mid); });
+      if (!C.sync()) return;
       {
-        int slot[2] = {0, 1};
-        tile_reduce<2>(C, slot, [&](int i, double (&v)[2]) {
-          double y[1];
-          spmv_row<1>(P.AP, P.p, i, y);
-          const double bb = P.bP[i];
-          const double df = y[0] - bb;
-          v[0] = df * df;
-          v[1] = bb * bb;
-        });
-        grid_each(P.nf, [&](int f) { P.pf[f] = face_scalar(P, P.p, f, P.bcP, mid); });
-        if (!C.sync()) return;
         double red[2];
-        final_sum<2>(P.part, slot, P.ntiles, C.sm, C.sm_out, red);
+        final_sum<2>(P.part, P.ntiles, C.sm, C.sm_out, red);
         Rit[3] = sqrt(red[0] / (double)P.n) / sqrt(red[1]);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
           P.R[(size_t)it * 4 + 3] = Rit[3];
@@ -920,13 +952,12 @@ __device__ void solve_program(Ctx &C) {
     krylov_init_row<1>(P, P.AU, P.wU, b, P.U, i, P.solve_solver);
   });
   if (!C.sync()) return;
-  {
-    const double *in = (P.solve_solver == SOLVER_BICGSTAB) ? P.wU.q : P.wU.r;
-    double *out = (P.solve_solver == SOLVER_BICGSTAB) ? P.wU.r : P.wU.v;
-    if (!precon_setup_apply<1>(C, P.AU, in, out, 0xffu)) return;
-  }
+  if (!krylov_start<1>(C, P.AU, P.wU, P.sb, P.solve_solver)) return;
   KCfg cfg;
-  cfg.solver = P.solve_solver; cfg.itmax = P.solve_itmax; cfg.atol = P.solve_atol; cfg.rtol = P.solve_rtol;
+  cfg.solver = P.solve_solver;
+  cfg.itmax = P.solve_itmax;
+  cfg.atol = P.solve_atol;
+  cfg.rtol = P.solve_rtol;
   int its[1];
   double rn[1];
   if (!krylov<1>(C, P.AU, P.wU, P.sb, cfg, P.solve_solver, its, rn)) return;
@@ -940,15 +971,17 @@ __device__ void solve_program(Ctx &C) {
 
 }  // namespace
 
+// KParams is passed by value: the fields live in the kernel's constant
+// parameter bank instead of occupying registers.
 template <int NS>
-__global__ void __launch_bounds__(TPB, 2) xcal_program_kernel(const KParams *__restrict__ pp, int prog, int iters) {
+__global__ void __launch_bounds__(TPB, 2) xcal_program_kernel(const __grid_constant__ KParams prm, int prog, int iters) {
   __shared__ double sm[8 * MAXK];
   __shared__ double sm_out[MAXK];
   __shared__ int sm_ok;
   Ctx C;
-  C.P = pp;
-  C.S.bar = pp->bar;
-  C.S.mode = pp->mode;
+  C.P = &prm;
+  C.S.bar = prm.bar;
+  C.S.mode = prm.mode;
   C.S.nb = gridDim.x;
   C.S.epoch = 0;
   C.S.ok = &sm_ok;
@@ -961,34 +994,27 @@ __global__ void __launch_bounds__(TPB, 2) xcal_program_kernel(const KParams *__r
   simple_program<NS>(C, iters, prog == PROG_PISO);
 }
 
-template __global__ void xcal_program_kernel<1>(const KParams *, int, int);
-template __global__ void xcal_program_kernel<2>(const KParams *, int, int);
-template __global__ void xcal_program_kernel<3>(const KParams *, int, int);
+template __global__ void xcal_program_kernel<1>(const __grid_constant__ KParams, int, int);
+template __global__ void xcal_program_kernel<2>(const __grid_constant__ KParams, int, int);
+template __global__ void xcal_program_kernel<3>(const __grid_constant__ KParams, int, int);
 
 // ------------------------------------------------------------ host launch
-static cudaError_t set_attrs(const void *fn, bool cluster) {
-  if (cluster) return cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  return cudaSuccess;
-}
-
 const void *program_kernel_ptr(int ns) {
   if (ns == 1) return (const void *)xcal_program_kernel<1>;
   if (ns == 2) return (const void *)xcal_program_kernel<2>;
   return (const void *)xcal_program_kernel<3>;
 }
 
-cudaError_t launch_program(int ns, int mode, int nblocks, const KParams *dparams, int prog, int iters,
+cudaError_t launch_program(int ns, int mode, int nblocks, const KParams *hparams, int prog, int iters,
                            cudaStream_t stream) {
   const void *fn = program_kernel_ptr(ns);
   void *args[3];
-  args[0] = (void *)&dparams;
+  args[0] = (void *)hparams;
   args[1] = (void *)&prog;
   args[2] = (void *)&iters;
-  if (mode == SYNC_BLOCK) {
-    return cudaLaunchKernel(fn, dim3(1), dim3(TPB), args, 0, stream);
-  }
+  if (mode == SYNC_BLOCK) return cudaLaunchKernel(fn, dim3(1), dim3(TPB), args, 0, stream);
   if (mode == SYNC_CLUSTER) {
-    cudaError_t e = set_attrs(fn, true);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nblocks);
@@ -1016,7 +1042,7 @@ int max_coresident_blocks(int ns, int device) {
 
 int max_cluster_blocks(int ns) {
   const void *fn = program_kernel_ptr(ns);
-  if (set_attrs(fn, true) != cudaSuccess) return 8;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 8;
   for (int c = 16; c >= 1; c >>= 1) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c);

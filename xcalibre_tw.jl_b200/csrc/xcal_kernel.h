@@ -5,7 +5,7 @@
 #include "xcal_device.cuh"
 
 namespace xcal {
-cudaError_t launch_program(int ns, int mode, int nblocks, const KParams *dparams, int prog, int iters,
+cudaError_t launch_program(int ns, int mode, int nblocks, const KParams *hparams, int prog, int iters,
                            cudaStream_t stream);
 int max_coresident_blocks(int ns, int device);
 int max_cluster_blocks(int ns);
