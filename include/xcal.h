@@ -219,6 +219,11 @@ int xcal_linear_solve(xcal_ctx ctx, int32_t solver, int32_t precon, int64_t n,
                       const double *b, double *x, int32_t itmax, double atol,
                       double rtol, int32_t *niter, double *final_rnorm);
 
+/* residual!(R, equation, phi): R = sqrt(mean((A*x - b)^2)) / norm(b) for a CSR
+ * system (0-based, columns ascending), src/Solvers/Solvers_0_functions.jl:13-63. */
+int xcal_residual(xcal_ctx ctx, int64_t n, const int32_t *row_ptr, const int32_t *col,
+                  const double *val, const double *x, const double *b, double *R);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,8 @@ def lib():
         L.orc_linear_solve.argtypes = [C.c_int32, C.c_int32, C.c_int64, P_i32, P_i32, P_d, P_d,
                                        P_d, C.c_int32, C.c_double, C.c_double, P_i32, P_d]
         L.orc_dilu_apply.argtypes = [C.c_int64, P_i32, P_i32, P_d, P_d, P_d, P_d]
+        L.orc_residual.argtypes = [C.c_int64, P_i32, P_i32, P_d, P_d, P_d]
+        L.orc_residual.restype = C.c_double
         L.orc_canon_dot.argtypes = [C.c_int64, P_d, P_d]
         L.orc_canon_dot.restype = C.c_double
         L.orc_levels.argtypes = [C.c_int64, P_i32, P_i32, P_i32, P_i32]
@@ -192,3 +194,13 @@ def levels(row_ptr, col):
     cl = np.ascontiguousarray(col, dtype=np.int32)
     lib().orc_levels(n, _abi.i32ptr(rp), _abi.i32ptr(cl), _abi.i32ptr(fl), _abi.i32ptr(bl))
     return fl, bl
+
+
+def residual(row_ptr, col, val, x, b):
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    vv = np.ascontiguousarray(val, dtype=np.float64)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    return lib().orc_residual(len(bb), _abi.i32ptr(rp), _abi.i32ptr(cl), _abi.dptr(vv), _abi.dptr(xx),
+                              _abi.dptr(bb))

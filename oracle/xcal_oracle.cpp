@@ -1480,6 +1480,25 @@ int orc_dilu_apply(int64_t n, const int32_t *rp, const int32_t *col, const doubl
   return XCAL_OK;
 }
 
+// residual!(R, equation, phi) on a CSR system (Solvers_0_functions.jl:13-63)
+double orc_residual(int64_t n, const int32_t *rp, const int32_t *col, const double *val, const double *x,
+                    const double *b) {
+  Eqn E;
+  E.A.n = n; E.A.colptr.assign(n + 1, 0);
+  for (i64 i = 0; i < n; ++i) for (int32_t q = rp[i]; q < rp[i + 1]; ++q) E.A.colptr[col[q] + 1]++;
+  for (i64 j = 0; j < n; ++j) E.A.colptr[j + 1] += E.A.colptr[j];
+  E.A.rowval.assign(E.A.colptr[n], 0); E.A.nzval.assign(E.A.colptr[n], 0.0);
+  std::vector<i64> fill(E.A.colptr.begin(), E.A.colptr.end() - 1);
+  for (i64 i = 0; i < n; ++i)
+    for (int32_t q = rp[i]; q < rp[i + 1]; ++q) {
+      i64 j = col[q], pos = fill[j]++;
+      E.A.rowval[pos] = i; E.A.nzval[pos] = val[q];
+    }
+  E.b.assign(b, b + n);
+  std::vector<double> xx(x, x + n);
+  return residual(E, xx);
+}
+
 double orc_canon_dot(int64_t n, const double *x, const double *y) {
   return canon_sum_f(n, [&](i64 i) { return x[i] * y[i]; });
 }

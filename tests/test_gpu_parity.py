@@ -148,3 +148,25 @@ def test_api_simple_end_to_end():
     Rx, Ry, Rp = X.simple(model, config, pref=pref)
     assert len(Rx) == 50 and np.isnan(Ry[0])   # 0/0 in the first uy residual, as in the reference
     assert np.all(np.isfinite(model.p.values)) and np.abs(model.U.x.values).max() > 0.1
+
+
+def test_residual_operator_parity():
+    """xcal_residual (residual! on a CSR system) against the oracle."""
+    import ctypes as C
+    rp, col, out = _snapshot_matrix(n=30, iters=4)
+    A = out["Ap"]
+    n = len(rp) - 1
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n)
+    b = rng.standard_normal(n)
+    ro = O.residual(rp, col, A, x, b)
+    lib = _abi.load()
+    h = C.c_void_p()
+    _abi.check(lib.xcal_ctx_create(0, 0, C.byref(h)))
+    try:
+        R = np.zeros(1)
+        _abi.check(lib.xcal_residual(h, n, _abi.i32ptr(rp), _abi.i32ptr(col), _abi.dptr(A), _abi.dptr(x),
+                                     _abi.dptr(b), _abi.dptr(R)), h)
+    finally:
+        lib.xcal_ctx_destroy(h)
+    assert R[0] == ro or abs(R[0] - ro) <= TOL * abs(ro)

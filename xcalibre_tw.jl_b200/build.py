@@ -17,7 +17,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
          "--expt-relaxed-constexpr"]
-SOURCES = ["xcal_kernel.cu", "xcal_api.cu", "host_mesh.cpp"]
+SOURCES = ["xcal_kernel.cu", "xcal_ops.cu", "xcal_api.cu", "host_mesh.cpp"]
 
 
 def build(verbose=False):

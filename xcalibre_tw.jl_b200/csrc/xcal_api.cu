@@ -14,6 +14,7 @@
 #include "../../include/xcal.h"
 #include "host_mesh.h"
 #include "xcal_kernel.h"
+#include "xcal_ops.h"
 
 using namespace xcal;
 
@@ -708,6 +709,42 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   if (niter) *niter = (int32_t)so[0];
   if (final_rnorm) *final_rnorm = so[1];
   if (bar.err) return fail(c, XCAL_ERR_TIMEOUT, "device barrier timed out");
+  return XCAL_OK;
+}
+
+// ------------------------------------------------------------- residual!
+static int check_csr(xcal_ctx c, int n, const int32_t *rp, const int32_t *col) {
+  if (rp[0] != 0) return fail(c, XCAL_ERR_ARG, "row_ptr[0] must be 0");
+  for (int i = 0; i < n; ++i) {
+    if (rp[i + 1] < rp[i]) return fail(c, XCAL_ERR_ARG, "row_ptr not monotone");
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      if (col[k] < 0 || col[k] >= n) return fail(c, XCAL_ERR_ARG, "column out of range");
+      if (k > rp[i] && col[k] <= col[k - 1]) return fail(c, XCAL_ERR_ARG, "columns not strictly ascending");
+    }
+  }
+  return XCAL_OK;
+}
+
+int xcal_residual(xcal_ctx c, int64_t n64, const int32_t *row_ptr, const int32_t *col, const double *val,
+                  const double *x, const double *b, double *R) {
+  if (!c || !row_ptr || !col || !val || !x || !b || !R || n64 <= 0 || n64 > (1 << 30)) return XCAL_ERR_ARG;
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  int n = (int)n64;
+  TRY(check_csr(c, n, row_ptr, col));
+  int nnz = row_ptr[n];
+  int ntiles = (n + TILE - 1) / TILE;
+  DevBuf B;
+  std::vector<int> rp(row_ptr, row_ptr + n + 1), cl(col, col + nnz);
+  std::vector<double> vv(val, val + nnz), xx(x, x + n), bb(b, b + n);
+  int *drp, *dcl;
+  double *dv, *dx, *db;
+  TRY(upload(c, B, drp, rp)); TRY(upload(c, B, dcl, cl)); TRY(upload(c, B, dv, vv));
+  TRY(upload(c, B, dx, xx)); TRY(upload(c, B, db, bb));
+  double *part = B.alloc<double>((size_t)2 * ntiles), *out = B.alloc<double>(1);
+  if (!part || !out) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+  CUDA_TRY(c, launch_residual(n, drp, dcl, dv, dx, db, part, out, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(R, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return XCAL_OK;
 }
 

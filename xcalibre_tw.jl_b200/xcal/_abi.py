@@ -126,6 +126,7 @@ SIGNATURES = {
     "xcal_linear_solve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int64, P_i32,
                                     P_i32, P_d, P_d, P_d, C.c_int32, C.c_double, C.c_double,
                                     P_i32, P_d]),
+    "xcal_residual": (C.c_int, [C.c_void_p, C.c_int64, P_i32, P_i32, P_d, P_d, P_d, P_d]),
 }
 
 _lib = None
