@@ -224,6 +224,19 @@ int xcal_linear_solve(xcal_ctx ctx, int32_t solver, int32_t precon, int64_t n,
 int xcal_residual(xcal_ctx ctx, int64_t n, const int32_t *row_ptr, const int32_t *col,
                   const double *val, const double *x, const double *b, double *R);
 
+/* Allocation-free residual!: for callers that cannot allocate device memory at
+ * the point of the call (a host framework that owns all device memory through
+ * its own pool, or a loop that must not pay cudaMalloc's device-wide
+ * synchronisation).  No counterpart in the reference.  Same result as
+ * xcal_residual, but all pointers are device memory (CSR 0-based, columns
+ * ascending; R receives one double) and the partial sums live in a fixed
+ * 1 MiB array of the library, so n is limited to 16,777,216 rows
+ * (XCAL_ERR_ARG beyond).  The first call on a device resolves that array's
+ * address: make it before any stream capture.  The call synchronises the
+ * context's stream; calls that overlap on the GPU share the array and race. */
+int xcal_residual_noalloc(xcal_ctx ctx, int64_t n, const int32_t *d_row_ptr, const int32_t *d_col,
+                          const double *d_val, const double *d_x, const double *d_b, double *d_R);
+
 #ifdef __cplusplus
 }
 #endif

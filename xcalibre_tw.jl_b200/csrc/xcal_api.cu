@@ -748,4 +748,25 @@ int xcal_residual(xcal_ctx c, int64_t n64, const int32_t *row_ptr, const int32_t
   return XCAL_OK;
 }
 
+// Allocation-free residual!: same kernels as xcal_residual, device pointers in
+// and out, partial sums in the library's fixed scratch array (no cudaMalloc,
+// cudaFree or other allocation).  The first call on a device resolves the
+// scratch address; make it before any stream capture.  Calls that overlap on
+// the GPU (other threads, other contexts) share the scratch and race.
+int xcal_residual_noalloc(xcal_ctx c, int64_t n64, const int32_t *d_row_ptr, const int32_t *d_col,
+                          const double *d_val, const double *d_x, const double *d_b, double *d_R) {
+  if (!c) return XCAL_ERR_ARG;
+  if (!d_row_ptr || !d_col || !d_val || !d_x || !d_b || !d_R) return fail(c, XCAL_ERR_ARG, "null device pointer");
+  if (n64 <= 0) return fail(c, XCAL_ERR_ARG, "n must be positive");
+  if (n64 > (int64_t)noalloc_max_rows())
+    return fail(c, XCAL_ERR_ARG, "n = " + std::to_string(n64) + " exceeds the allocation-free limit of " +
+                                     std::to_string(noalloc_max_rows()) + " rows");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  double *scratch = nullptr;
+  CUDA_TRY(c, noalloc_scratch(c->device, &scratch));
+  CUDA_TRY(c, launch_residual((int)n64, d_row_ptr, d_col, d_val, d_x, d_b, scratch, d_R, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return XCAL_OK;
+}
+
 }  // extern "C"

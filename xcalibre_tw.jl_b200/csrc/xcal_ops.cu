@@ -3,8 +3,11 @@
 // xcal_residual: residual!(R, equation, phi) (src/Solvers/Solvers_0_functions.jl:13-63),
 //   R = sqrt(mean((A*x - b)^2)) / norm(b), with the SpMV in ascending column order
 //   and the canonical reduction of xcal_device.cuh.
+// xcal_residual_noalloc: the same kernels for callers that must not allocate
+//   device memory, with the per-tile partial sums in a fixed file-scope array.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -57,5 +60,33 @@ cudaError_t launch_residual(int n, const int *rp, const int *col, const double *
   residual_final_kernel<<<1, TPB, 0, stream>>>(n, part, ntiles, out);
   return cudaGetLastError();
 }
+
+// ------------------------------------------------ allocation-free variant
+// Scratch of xcal_residual_noalloc: two partial sums per 256-row tile, for at
+// most XCAL_NOALLOC_MAX_TILES tiles (16,777,216 rows), 1 MiB on every device
+// that loads the library, kept until the process exits.  All calls share it.
+constexpr int XCAL_NOALLOC_MAX_TILES = 65536;
+constexpr int XCAL_NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) double g_noalloc_partials[2 * XCAL_NOALLOC_MAX_TILES];
+
+// Device address of the scratch, resolved once per device with that device
+// current (in host code the symbol names a host-side stand-in, not device memory).
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[XCAL_NOALLOC_MAX_DEVICES] = {};
+
+cudaError_t noalloc_scratch(int device, double **out) {
+  if (device < 0 || device >= XCAL_NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = (double *)p;
+  }
+  *out = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+
+int noalloc_max_rows() { return XCAL_NOALLOC_MAX_TILES * TILE; }
 
 }  // namespace xcal

@@ -127,6 +127,8 @@ SIGNATURES = {
                                     P_i32, P_d, P_d, P_d, C.c_int32, C.c_double, C.c_double,
                                     P_i32, P_d]),
     "xcal_residual": (C.c_int, [C.c_void_p, C.c_int64, P_i32, P_i32, P_d, P_d, P_d, P_d]),
+    "xcal_residual_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
