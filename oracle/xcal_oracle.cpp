@@ -1051,11 +1051,13 @@ static int run_solver(const OMesh &M, const xcal_case &cfg, bool piso, int itera
   // k-omega initialise_RANS: RANSModels_kOmega.jl:172-234
   Vec nutf(nf, 0.0), nueffk(nf, 0.0), nueffw(nf, 0.0), Dkf(nc, 0.0), Dwf(nc, 0.0), Pk(nc, 0.0), Pw(nc, 0.0);
   Vec G[9];
-  Eqn keq, weq; Terms TK, TW; Precon PK, PW;
+  // k_eqn and omega_eqn are built on p_eqn.equation (initialise_RANS, :178-207):
+  // one storage for the three systems, as in the reference
+  Eqn &keq = peq, &weq = peq;
+  Terms TK, TW; Precon PK, PW;
   const double bplus = 0.09, alpha1 = 0.52, beta1c = 0.072, sigk = 0.5, sigw = 0.5;   // get_coeffs :152-160
   if (turb) {
     for (int i = 0; i < 9; ++i) G[i].assign(nc, 0.0);
-    build_pattern(M, keq.A); keq.b.assign(nc, 0.0); build_pattern(M, weq.A); weq.b.assign(nc, 0.0);
     TK.has_time = true; TK.time = cfg.schemes_k.time; TK.dt = cfg.dt;
     TK.has_div = true; TK.div = cfg.schemes_k.divergence; TK.mdot = &mdotf;
     TK.has_lap = true; TK.lap_sign = -1; TK.gamma = &nueffk; TK.has_si = true; TK.si = &Dkf;

@@ -28,7 +28,14 @@ def run_device(mesh, model, config, pref, iterations, renumber, piso=False):
         U, p = cases.fields(model)
         s.set_field(_abi.FIELD_UX, U[0]); s.set_field(_abi.FIELD_UY, U[1]); s.set_field(_abi.FIELD_UZ, U[2])
         s.set_field(_abi.FIELD_P, p)
+        if X.isturbulent(model):
+            t = model.turbulence
+            s.set_field(_abi.FIELD_K, t.k.values); s.set_field(_abi.FIELD_OMEGA, t.omega.values)
+            s.set_field(_abi.FIELD_NUT, t.nut.values)
         out = s.run(iterations, piso=piso)
+        if X.isturbulent(model):
+            out["k"] = s.get_field(_abi.FIELD_K); out["omega"] = s.get_field(_abi.FIELD_OMEGA)
+            out["nut"] = s.get_field(_abi.FIELD_NUT)
         out["U"] = np.stack([s.get_field(_abi.FIELD_UX), s.get_field(_abi.FIELD_UY), s.get_field(_abi.FIELD_UZ)])
         out["p"] = s.get_field(_abi.FIELD_P)
         out["perm"] = s.permutation() - 1
@@ -52,9 +59,18 @@ def run_oracle(dev_mesh, model, config, pref, iterations, perm, piso=False):
     Ud[:, perm] = U
     pd[perm] = p
     om = O.from_mesh2(dev_mesh)
-    out = O.run(om, case, iterations, Ud, pd, piso=piso, ref_cell=int(perm[0]), want_eqns=True)
+    extra = {}
+    if X.isturbulent(model):
+        t = model.turbulence
+        for name, f in (("k", t.k.values), ("omega", t.omega.values), ("nut", t.nut.values)):
+            v = np.zeros_like(p)
+            v[perm] = f
+            extra[name] = v
+    out = O.run(om, case, iterations, Ud, pd, piso=piso, ref_cell=int(perm[0]), want_eqns=True, **extra)
     out["U"] = out["U"][:, perm]
     out["p"] = out["p"][perm]
+    for name in extra:
+        out[name] = out[name][perm]
     return out
 
 
@@ -66,6 +82,9 @@ def compare(dev, orc, nU=2, check_eqns=True):
     for d in range(nU):
         r[f"U{d}"] = rel_l2(dev["U"][d], orc["U"][d])
     r["p"] = rel_l2(dev["p"], orc["p"])
+    for name in ("k", "omega", "nut"):
+        if name in dev:
+            r[name] = rel_l2(dev[name], orc[name])
     if check_eqns:
         r["AU"] = rel_l2(dev["AU"], orc["AU"])
         r["Ap"] = rel_l2(dev["Ap"], orc["Ap"])

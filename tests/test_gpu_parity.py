@@ -170,3 +170,23 @@ def test_residual_operator_parity():
     finally:
         lib.xcal_ctx_destroy(h)
     assert R[0] == ro or abs(R[0] - ro) <= TOL * abs(ro)
+
+
+def test_komega_flatplate_parity():
+    """k-omega (turbulence!, omega wall function) on a coarse graded flat plate."""
+    mesh, model, config, pref = cases.flatplate(60, 30, iterations=40)
+    dev = run_device(mesh, model, config, pref, 40, _abi.RENUMBER_COLOR)
+    orc = run_oracle(dev["dev_mesh"], model, config, pref, 40, dev["perm"])
+    d = assert_parity(dev, orc)
+    print("komega", d)
+
+
+def test_komega_wall_functions_parity():
+    """k and nut wall functions (correct_production!, correct_nut_wall!): their
+    log() comes from CUDA on the device and from libm in the oracle, so the
+    comparison uses the FP64 tolerance rather than bit equality."""
+    mesh, model, config, pref = cases.flatplate(60, 30, iterations=30, wall_functions=True)
+    dev = run_device(mesh, model, config, pref, 30, _abi.RENUMBER_COLOR)
+    orc = run_oracle(dev["dev_mesh"], model, config, pref, 30, dev["perm"])
+    d = assert_parity(dev, orc)
+    print("komega-wf", d)

@@ -364,6 +364,11 @@ static int build_bc(xcal_ctx c, DevBuf &B, const xcal_bc *bcs, int nbc, FieldBC 
     e.type = x.type; e.pad = 0;
     for (int d = 0; d < 3; ++d) e.v[d] = vector ? x.value[d] : x.value[0];
     e.kappa = x.kappa; e.beta1 = x.beta1; e.cmu = x.cmu; e.B = x.B; e.E = x.E;
+    // y_plus_laminar(E, kappa) and cmu^0.25 (RANSModels_kOmega.jl:322-331), host libm
+    double yl = 11.0;
+    for (int it = 0; it < 10; ++it) yl = std::log(std::max(yl * x.E, 1.0)) / x.kappa;
+    e.ylam = yl;
+    e.c25 = std::pow(x.cmu, 0.25);
     for (int64_t k = M.pptr[x.patch]; k < M.pptr[x.patch + 1]; ++k) {
       cnt[M.pcells[k] + 1]++;
       fbc[M.pfaces[k]] = b;
@@ -401,7 +406,14 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   if (!c || !cfg) return XCAL_ERR_ARG;
   if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_case_setup before xcal_mesh_upload");
   CUDA_TRY(c, cudaSetDevice(c->device));
-  if (cfg->model != XCAL_MODEL_LAMINAR) return fail(c, XCAL_ERR_UNSUPPORTED, "turbulence model not available on the device path");
+  if (cfg->model != XCAL_MODEL_LAMINAR && cfg->model != XCAL_MODEL_KOMEGA) return fail(c, XCAL_ERR_ARG, "unknown model");
+  const bool turb = (cfg->model == XCAL_MODEL_KOMEGA);
+  if (turb) {
+    TRY(check_solver(c, cfg->solver_k, "k"));
+    TRY(check_solver(c, cfg->solver_omega, "omega"));
+    if (!(cfg->solver_k.relax > 0.0) || !(cfg->solver_omega.relax > 0.0)) return fail(c, XCAL_ERR_ARG, "relaxation factors must be > 0");
+    if (c->ns == 3) return fail(c, XCAL_ERR_UNSUPPORTED, "k-omega is a 2D model in the reference");
+  }
   if (cfg->precision != XCAL_PREC_FP64) return fail(c, XCAL_ERR_UNSUPPORTED, "mixed precision not available");
   TRY(check_solver(c, cfg->solver_U, "U"));
   TRY(check_solver(c, cfg->solver_p, "p"));
@@ -417,6 +429,19 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   size_t nnz = (size_t)c->prep.W * c->prep.np;
   TRY(build_bc(c, B, cfg->bc_U, cfg->nbc_U, h.bcU, c->tabU, true, "U"));
   TRY(build_bc(c, B, cfg->bc_p, cfg->nbc_p, h.bcP, c->tabP, false, "p"));
+  h.model = cfg->model;
+  if (turb) {
+    std::vector<BcEntry> tk, tw, tn;
+    TRY(build_bc(c, B, cfg->bc_k, cfg->nbc_k, h.bcK, tk, false, "k"));
+    TRY(build_bc(c, B, cfg->bc_omega, cfg->nbc_omega, h.bcW, tw, false, "omega"));
+    TRY(build_bc(c, B, cfg->bc_nut, cfg->nbc_nut, h.bcN, tn, false, "nut"));
+    h.kK.solver = cfg->solver_k.solver; h.kK.itmax = cfg->solver_k.itmax; h.kK.atol = cfg->solver_k.atol; h.kK.rtol = cfg->solver_k.rtol;
+    h.kW.solver = cfg->solver_omega.solver; h.kW.itmax = cfg->solver_omega.itmax; h.kW.atol = cfg->solver_omega.atol; h.kW.rtol = cfg->solver_omega.rtol;
+    h.precK = cfg->solver_k.preconditioner; h.precW = cfg->solver_omega.preconditioner;
+    h.divK = cfg->schemes_k.divergence; h.divW = cfg->schemes_omega.divergence;
+    h.timeK = cfg->schemes_k.time; h.timeW = cfg->schemes_omega.time;
+    h.aK = cfg->solver_k.relax; h.aW = cfg->solver_omega.relax;
+  }
   h.div = cfg->schemes_U.divergence; h.time = cfg->schemes_U.time; h.grad = cfg->schemes_p.gradient;
   h.dt = cfg->dt; h.nu = cfg->nu; h.aU = cfg->solver_U.relax; h.aP = cfg->solver_p.relax;
   h.has_pref = cfg->has_pref ? 1 : 0; h.pref = cfg->pref;
@@ -438,9 +463,19 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
     for (int b = 0; b < 2; ++b) { w->r[b] = A(m); w->p[b] = A(m); w->v[b] = A(m); }
   }
   h.part = A((size_t)MAXK * h.ntiles);
+  if (turb) {
+    h.k = A(n); h.w = A(n); h.nut = A(n); h.nutf = A(nf); h.nueffk = A(nf); h.nueffw = A(nf);
+    h.Dk = A(n); h.Dw = A(n); h.Pk = A(n); h.Pw = A(n); h.G = A((size_t)n * 9);
+  }
   h.bar = B.alloc<Bar>(1);
   h.done = B.alloc<int>(1);
   if (!ok || !h.bar || !h.done) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+  if (turb) {
+    CUDA_TRY(c, cudaMemsetAsync(h.k, 0, sizeof(double) * n, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(h.w, 0, sizeof(double) * n, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(h.nut, 0, sizeof(double) * n, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(h.nutf, 0, sizeof(double) * nf, c->stream));
+  }
   // fields start at zero (ScalarField/VectorField constructors)
   CUDA_TRY(c, cudaMemsetAsync(h.U, 0, sizeof(double) * n * NS, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(h.Uz2, 0, sizeof(double) * n, c->stream));
@@ -476,7 +511,12 @@ static int field_target(xcal_ctx c, int32_t field, double *&base, int &stride, i
       if (NS == 3) { base = h.U; stride = 3; off = 2; } else { base = h.Uz2; stride = 1; off = 0; }
       return XCAL_OK;
     case XCAL_FIELD_P: base = h.p; stride = 1; off = 0; return XCAL_OK;
-    default: return fail(c, XCAL_ERR_UNSUPPORTED, "field not available on the laminar device path");
+    case XCAL_FIELD_K: case XCAL_FIELD_OMEGA: case XCAL_FIELD_NUT:
+      if (h.model != XCAL_MODEL_KOMEGA) return fail(c, XCAL_ERR_STATE, "turbulence fields need the k-omega model");
+      base = (field == XCAL_FIELD_K) ? h.k : (field == XCAL_FIELD_OMEGA) ? h.w : h.nut;
+      stride = 1; off = 0;
+      return XCAL_OK;
+    default: return fail(c, XCAL_ERR_ARG, "unknown field");
   }
 }
 

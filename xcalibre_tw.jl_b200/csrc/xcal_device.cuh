@@ -39,6 +39,7 @@ struct BcEntry {
   int pad;
   double v[3];
   double kappa, beta1, cmu, B, E;
+  double ylam, c25;   // wall functions: y_plus_laminar(E, kappa) and cmu^0.25, computed on the host
 };
 
 // Boundary conditions of one field, device form.
@@ -92,6 +93,13 @@ struct KParams {
   int has_pref, ref_cell;
   double pref;
   KCfg kU, kP;
+  // k-omega (RANSModels_kOmega.jl); k and omega reuse the pressure system's storage
+  int model;
+  double *k, *w, *nut, *nutf, *nueffk, *nueffw, *Dk, *Dw, *Pk, *Pw, *G;   // G [n*9] grad U
+  FieldBC bcK, bcW, bcN;
+  KCfg kK, kW;
+  int precK, precW, divK, divW, timeK, timeW;
+  double aK, aW;
   // state
   double *U, *Uz2;      // U [n*NS] interleaved; Uz2: z component kept for 2D meshes
   double *p, *gp, *bU, *bP, *H, *rD, *divH;

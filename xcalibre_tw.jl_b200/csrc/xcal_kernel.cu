@@ -708,6 +708,9 @@ template <int NS>
 __device__ __forceinline__ void face_mdot(const KParams &P, int f) {
   double u[NS];
   face_vector<NS>(P, P.U, f, u);
+  if (P.model == 1)
+#pragma unroll
+    for (int d = 0; d < NS; ++d) P.UfH[(size_t)f * NS + d] = u[d];
   const double a = __ldg(P.area + f);
   double m = u[0] * (a * __ldg(P.fnx + f)) + u[1] * (a * __ldg(P.fny + f));
   if (NS == 3) m = m + u[2] * (a * __ldg(P.fnz + f));
@@ -799,6 +802,285 @@ __device__ bool gradient_p(Ctx &C, bool correct_u) {
   return true;
 }
 
+// ------------------------------------------------------------- k-omega
+// Wilcox k-omega of RANSModels_kOmega.jl:114-415 and RANSModels_functions.jl:5-88.
+constexpr double KW_BPLUS = 0.09, KW_ALPHA1 = 0.52, KW_BETA1 = 0.072, KW_SIGK = 0.5, KW_SIGW = 0.5;   // get_coeffs
+
+__device__ __forceinline__ double nut_wall_fn(double nu, double yplus, double kappa, double E) {
+  return jmax(nu * (yplus * kappa / log(jmax(E * yplus, 1.0 + 1e-4)) - 1), 0.0);
+}
+
+// omega of a wall cell (constraint!/set_cell_value!, :364-448)
+__device__ __forceinline__ double omega_wall(const KParams &P, const BcEntry &e, double kc, double y) {
+  const double wvis = 6.0 * P.nu / (e.beta1 * (y * y));
+  const double wlog = sqrt(kc) / (e.c25 * e.kappa * y);
+  const double yplus = e.c25 * y * sqrt(kc) / P.nu;
+  return (yplus > e.ylam) ? wlog : wvis;
+}
+
+// Transport row of k or omega: Time + Divergence(mdotf) - Laplacian(nueff) +
+// Si(D) == Source(P) (:191-207) with BCs (Discretise_3_boundary_conditions.jl),
+// implicit_relaxation! and, for omega, constrain_equation! (:346-399).
+__device__ __forceinline__ double scalar_row(const KParams &P, const Mat &A, int i, const double *phi,
+                                             const double *gam, const double *Si, const double *src,
+                                             const FieldBC &bc, double alpha, int div, int time, bool omega) {
+  const double vol = __ldg(P.vol + i);
+  double acc = 0.0;
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    const double ns = (double)__ldg(P.f_sign + e);
+    const int pos = __ldg(P.f_pos + e);
+    double t2;
+    const double mf = P.mdot[f];
+    if (div == DIV_UPWIND) {
+      const double ap = 1.0 * (mf * ns);
+      acc += jmax(ap, 0.0);
+      t2 = -jmax(-ap, 0.0);
+    } else {
+      const int nb = __ldg(P.f_nbr + e);
+      const double ax = __ldg(P.fcx + f) - __ldg(P.ccx + i), ay = __ldg(P.fcy + f) - __ldg(P.ccy + i),
+                   az = __ldg(P.fcz + f) - __ldg(P.ccz + i);
+      const double bx = __ldg(P.ccx + nb) - __ldg(P.ccx + i), by = __ldg(P.ccy + nb) - __ldg(P.ccy + i),
+                   bz = __ldg(P.ccz + nb) - __ldg(P.ccz + i);
+      const double weight = sqrt((ax * ax + ay * ay) + az * az) / sqrt((bx * bx + by * by) + bz * bz);
+      const double omw = 1.0 - weight;
+      const double ap = 1.0 * (mf * ns);
+      acc += ap * omw;
+      t2 = ap * weight;
+    }
+    const double ap3 = -1.0 * ((-gam[f]) * __ldg(P.area + f)) / __ldg(P.delta + f);
+    acc += ap3;
+    const double t3 = -ap3;
+    const double base = __ldg(P.f_first + e) ? 0.0 : A.val[pos];
+    A.val[pos] = (base + t2) + t3;
+  }
+  const double prev = phi[i];
+  double b = 0.0;
+  if (time == TIME_EULER) {
+    const double rdt = 1 / P.dt;
+    acc += vol * rdt;
+    b += prev * vol * rdt;
+  }
+  acc += 1.0 * Si[i] * vol;
+  b += 1.0 * src[i] * vol;
+  for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
+    const int f = __ldg(bc.a_face + q);
+    const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+    const double ap = 1.0 * P.mdot[f];
+    const bool neu = (e.type == BC_NEUMANN || e.type == BC_KWALL || e.type == BC_OMEGAWALL);
+    if (div == DIV_UPWIND) {
+      if (e.type == BC_DIRICHLET) b -= ap * e.v[0];
+      else if (neu) acc += jmax(ap, 0.0);
+    } else {
+      if (e.type == BC_DIRICHLET) b += 1.0 * ((-P.mdot[f]) * e.v[0]);
+      else if (neu) acc += ap;
+    }
+    if (e.type == BC_DIRICHLET) {
+      const double flux = gam[f] * __ldg(P.area + f) / __ldg(P.delta + f);
+      const double apl = -1.0 * (-flux);
+      acc += apl;
+      b += apl * e.v[0];
+    }
+    if (e.type == BC_OMEGAWALL) {
+      const double flux = 1.0 * Si[i];
+      b += flux * phi[i] * vol;
+    }
+  }
+  acc /= alpha;
+  b += (1.0 - alpha) * acc * prev;
+  if (omega)
+    for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
+      const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+      if (e.type != BC_OMEGAWALL) continue;
+      const double wc = omega_wall(P, e, P.k[i], __ldg(P.delta + __ldg(bc.a_face + q)));
+      b += acc * wc;
+      acc += acc;
+    }
+  A.val[__ldg(A.dpos + i)] = acc;
+  return b;
+}
+
+// grad!(gradU, Uf, U) Orthogonal (Calculate_0_gradient.jl:106-112) for cell i:
+// g[d][j] = dU_d/dx_j by Green-Gauss of the face values in UfH.
+template <int NS>
+__device__ __forceinline__ void grad_u_row(const KParams &P, int i, double (&g)[3][3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) g[d][j] = 0.0;
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    const double ns = (double)__ldg(P.f_sign + e);
+    const double a = __ldg(P.area + f);
+    const double sx = (a * __ldg(P.fnx + f)) * ns, sy = (a * __ldg(P.fny + f)) * ns, sz = (a * __ldg(P.fnz + f)) * ns;
+#pragma unroll
+    for (int d = 0; d < NS; ++d) {
+      const double v = P.UfH[(size_t)f * NS + d];
+      g[d][0] += v * sx;
+      g[d][1] += v * sy;
+      if (NS == 3) g[d][2] += v * sz;
+    }
+  }
+  const double vol = __ldg(P.vol + i);
+#pragma unroll
+  for (int d = 0; d < NS; ++d)
+#pragma unroll
+    for (int j = 0; j < NS; ++j) g[d][j] /= vol;
+  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q) {
+    const int f = __ldg(P.cb_face + q);
+    const double a = __ldg(P.area + f);
+    const double sx = a * __ldg(P.fnx + f), sy = a * __ldg(P.fny + f), sz = a * __ldg(P.fnz + f);
+#pragma unroll
+    for (int d = 0; d < NS; ++d) {
+      const double v = P.UfH[(size_t)f * NS + d];
+      double bx = v * sx, by = v * sy;
+      bx /= vol;
+      by /= vol;
+      g[d][0] += bx;
+      g[d][1] += by;
+      if (NS == 3) {
+        double bz = v * sz;
+        bz /= vol;
+        g[d][2] += bz;
+      }
+    }
+  }
+}
+
+// bound!(field, eps()) for the rows of forward level l: the reference's
+// sequential loop (later cells see updated values) in level order.
+__device__ __forceinline__ void bound_row(const KParams &P, double *fld, int i) {
+  const double EPS = 2.220446049250313e-16;
+  double sum_flux = 0.0;
+  int cnt = 0;
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    if (__ldg(P.f_face + e) < 0) break;
+    sum_flux += jmax(fld[__ldg(P.f_nbr + e)], EPS);
+    cnt += 1;
+  }
+  const double average = sum_flux / (double)cnt;
+  const double fi = fld[i];
+  fld[i] = jmax(jmax(fi, average * (signbit(fi) ? 1.0 : 0.0)), EPS);
+}
+
+template <int NS>
+__device__ bool turbulence(Ctx &C) {
+  const KParams &P = *C.P;
+  const double nu = P.nu;
+  // production, destruction, effective diffusivities (turbulence!, :256-272)
+  tile_each(P, [&](int i) {
+    double g[3][3];
+    grad_u_row<NS>(P, i, g);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P.G[(size_t)i * 9 + 3 * d + j] = g[d][j];
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < NS; ++j)
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const double Sjk = 0.5 * (g[k][j] + g[j][k]);
+        s += Sjk * Sjk;
+      }
+    const double pk = s * 2.0;
+    P.Pw[i] = KW_ALPHA1 * pk;
+    const double wi = P.w[i];
+    P.Dw[i] = KW_BETA1 * wi;
+    P.Dk[i] = KW_BPLUS * wi;
+    double pki = P.nut[i] * pk;
+    const FieldBC &bc = P.bcK;
+    for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {   // correct_production!
+      const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+      if (e.type != BC_KWALL) continue;
+      const int f = __ldg(bc.a_face + q);
+      const double delta = __ldg(P.delta + f);
+      const double nx = __ldg(P.fnx + f), ny = __ldg(P.fny + f), nz = __ldg(P.fnz + f);
+      const double kc = P.k[i];
+      const double uStar = e.c25 * sqrt(kc);
+      const double dUdy = uStar / (e.kappa * delta);
+      const double yplus = e.c25 * delta * sqrt(kc) / nu;
+      const double nutw = nut_wall_fn(nu, yplus, e.kappa, e.E);
+      const double ux = P.U[(size_t)i * NS] - 0.0, uy = P.U[(size_t)i * NS + 1] - 0.0;
+      const double uz = (NS == 3 ? P.U[(size_t)i * NS + 2] : P.Uz2[i]) - 0.0;
+      const double dn = (ux * nx + uy * ny) + uz * nz;
+      const double gx = (ux - nx * dn) / delta, gy = (uy - ny * dn) / delta, gz = (uz - nz * dn) / delta;
+      const double mag = sqrt((gx * gx + gy * gy) + gz * gz);
+      if (yplus > e.ylam) pki = (nu + nutw) * mag * dUdy;
+    }
+    P.Pk[i] = pki;
+  });
+  grid_each(P.nf, [&](int f) {
+    P.nueffw[f] = nu + KW_SIGW * P.nutf[f];
+    P.nueffk[f] = nu + KW_SIGK * P.nutf[f];
+  });
+  if (!C.sync()) return false;
+  for (int eq = 0; eq < 2; ++eq) {   // omega first, then k
+    const bool om = (eq == 0);
+    Mat A = P.AP;
+    A.precon = om ? P.precW : P.precK;
+    double *phi = om ? P.w : P.k;
+    const KCfg &cfg = om ? P.kW : P.kK;
+    tile_each(P, [&](int i) {
+      double b[1];
+      b[0] = om ? scalar_row(P, A, i, phi, P.nueffw, P.Dw, P.Pw, P.bcW, P.aW, P.divW, P.timeW, true)
+                : scalar_row(P, A, i, phi, P.nueffk, P.Dk, P.Pk, P.bcK, P.aK, P.divK, P.timeK, false);
+      P.bP[i] = b[0];
+      krylov_init_row<1>(P, A, P.wP, b, phi, i, cfg.solver);
+    });
+    if (!C.sync()) return false;
+    if (!krylov_start<1>(C, A, P.wP, P.bP, cfg.solver)) return false;
+    int its[1];
+    double rn[1];
+    if (!krylov<1>(C, A, P.wP, P.bP, cfg, cfg.solver, its, rn)) return false;
+    // run! copy-back, then constrain_boundary! for omega (:401-448)
+    tile_each(P, [&](int i) {
+      double v = P.wP.x[i] + phi[i];
+      if (om) {
+        const FieldBC &bc = P.bcW;
+        for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
+          const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+          if (e.type != BC_OMEGAWALL) continue;
+          v = omega_wall(P, e, P.k[i], __ldg(P.delta + __ldg(bc.a_face + q)));
+        }
+      }
+      phi[i] = v;
+    });
+    if (!C.sync()) return false;
+    for (int l = 0; l < P.nfl; ++l) {   // bound!(phi, eps()); after k also nut = k/omega
+      tile_each(P, [&](int i) {
+        if (__ldg(P.flev + i) != l) return;
+        bound_row(P, phi, i);
+        if (!om) P.nut[i] = P.k[i] / P.w[i];
+      });
+      if (!C.sync()) return false;
+    }
+  }
+  // interpolate!(nutf, nut) + correct_boundaries! + correct_eddy_viscosity! (:496-536)
+  // and update_nueff! (Solvers_0_functions.jl:1-11)
+  grid_each(P.nf, [&](int f) {
+    double v = face_scalar(P, P.nut, f, P.bcN, false);
+    if (f < P.nbf) {
+      const int bi = __ldg(P.bcN.fbc + f);
+      if (bi >= 0 && P.bcN.tab[bi].type == BC_NUTWALL) {
+        const BcEntry &e = P.bcN.tab[bi];
+        const int c = __ldg(P.o1 + f);
+        const double yplus = e.c25 * __ldg(P.delta + f) * sqrt(P.k[c]) / nu;
+        const double nutw = nut_wall_fn(nu, yplus, e.kappa, e.E);
+        if (yplus > e.ylam) v = nutw;
+      }
+    }
+    P.nutf[f] = v;
+    P.nueff[f] = nu + v;
+  });
+  return C.sync();
+}
+
 // ------------------------------------------------------------- programs
 template <int NS>
 __device__ void simple_program(Ctx &C, int iters, bool piso) {
@@ -809,7 +1091,8 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
   grid_each(P.nf, [&](int f) {
     face_mdot<NS>(P, f);
     P.pf[f] = face_scalar(P, P.p, f, P.bcP, mid);
-    P.nueff[f] = nu;
+    if (P.model == 1) P.nutf[f] = 0.0;   // initialise_RANS: a fresh face field
+    P.nueff[f] = (P.model == 1) ? nu + 0.0 : nu;
   });
   if (!C.sync()) return;
   if (!gradient_p<NS>(C, false)) return;
@@ -930,6 +1213,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       // interpolate!(Uf, U) + correct_boundaries! + flux!(mdotf, Uf)
       grid_each(P.nf, [&](int f) { face_mdot<NS>(P, f); });
       if (!C.sync()) return;
+      if (P.model == 1 && !turbulence<NS>(C)) return;
     }
     if (!piso) {
       // convergence test (Solvers_1_SIMPLE.jl:200-215); every CTA holds the

@@ -94,3 +94,41 @@ def fields(model):
     n = model.mesh.ncells
     U = np.stack([model.U.x.values, model.U.y.values, model.U.z.values])
     return U.reshape(3, n).copy(), model.p.values.copy()
+
+
+def flatplate(nx=600, ny=250, iterations=3000, wall_functions=False, **kw):
+    """k-omega flat plate 1 m x 0.2 m, U = 10 m/s, nu = 1.5e-5, inlet k from 1 %
+    intensity (0.015) and omega from a viscosity ratio of 10 (100); BCs as the
+    reference's low-Re flat-plate case (omega wall function on the plate).  With
+    wall_functions, k and nut also use their wall functions on the plate."""
+    path = _unv("flatplate", meshgen.flatplate_unv, nx=nx, ny=ny)
+    mesh = X.build_mesh(path)
+    model = X.RANS(X.KOmega, mesh=mesh, viscosity=X.ConstantScalar(1.5e-5))
+    Uin, kin = 10.0, 1.5 * (0.01 * 10.0) ** 2
+    win = kin / (10 * 1.5e-5)
+    X.assign(model, "U", X.Dirichlet("inlet", [Uin, 0.0, 0.0]), X.Neumann("outlet", 0.0),
+             X.Dirichlet("wall", [0.0, 0.0, 0.0]), X.Neumann("top", 0.0))
+    X.assign(model, "p", X.Neumann("inlet", 0.0), X.Dirichlet("outlet", 0.0), X.Neumann("wall", 0.0),
+             X.Neumann("top", 0.0))
+    X.assign(model, "turbulence.k", X.Dirichlet("inlet", kin), X.Neumann("outlet", 0.0),
+             X.KWallFunction("wall") if wall_functions else X.Dirichlet("wall", 0.0), X.Neumann("top", 0.0))
+    X.assign(model, "turbulence.omega", X.Dirichlet("inlet", win), X.Neumann("outlet", 0.0),
+             X.OmegaWallFunction("wall"), X.Neumann("top", 0.0))
+    X.assign(model, "turbulence.nut", X.Dirichlet("inlet", kin / win), X.Neumann("outlet", 0.0),
+             X.NutWallFunction("wall") if wall_functions else X.Dirichlet("wall", 0.0), X.Neumann("top", 0.0))
+    up = dict(divergence=X.Upwind)
+    schemes = dict(U=X.set_schemes(**up), p=X.set_schemes(**up), k=X.set_schemes(**up),
+                   omega=X.set_schemes(**up))
+    s = solvers_for(model, relax_u=0.8, relax_p=0.2, **kw)
+    s["k"] = X.set_solver(model.turbulence.k, solver=X.BicgstabSolver, preconditioner=X.DILU(),
+                          convergence=1e-7, relax=0.8)
+    s["omega"] = X.set_solver(model.turbulence.omega, solver=X.BicgstabSolver, preconditioner=X.DILU(),
+                              convergence=1e-7, relax=0.8)
+    config = X.Configuration(solvers=s, schemes=schemes,
+                             runtime=X.set_runtime(iterations=iterations, write_interval=-1, time_step=1))
+    X.initialise(model.U, [Uin, 0.0, 0.0])
+    X.initialise(model.p, 0.0)
+    X.initialise(model.turbulence.k, kin)
+    X.initialise(model.turbulence.omega, win)
+    X.initialise(model.turbulence.nut, kin / win)
+    return mesh, model, config, None
