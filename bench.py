@@ -39,6 +39,10 @@ def parse():
     ap.add_argument("--impl", default="xcal", choices=["xcal", "reference"])
     ap.add_argument("--config", default="bfs", choices=["bfs", "cavity", "cavity3d"])
     ap.add_argument("--renumber", default="color", choices=["color", "rcm", "none"])
+    ap.add_argument("--size", type=int, default=None,
+                    help="bfs: cells per step height (27); cavity: cells per side (40); cavity3d: cells per side (128)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 Krylov on FP64 assembly with FP64 residual refinement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-flush", action="store_true")
@@ -46,24 +50,29 @@ def parse():
     return ap.parse_args()
 
 
-def build_case(name):
+def build_case(name, size=None):
     from xcal import cases
     if name == "bfs":
-        mesh, model, config, pref = cases.bfs(27, iterations=2000)
-        desc = "laminar backward-facing step h=10mm, 27 cells/h, graded 1.05, jittered 10%, Re=50"
+        size = size or 27
+        mesh, model, config, pref = cases.bfs(size, iterations=2000)
+        desc = f"laminar backward-facing step h=10mm, {size} cells/h, graded 1.05, jittered 10%, Re=50"
     elif name == "cavity":
-        mesh, model, config, pref = cases.cavity2d(40, iterations=1000)
-        desc = "2D lid-driven cavity 40x40, Re=100"
+        size = size or 40
+        mesh, model, config, pref = cases.cavity2d(size, iterations=1000)
+        desc = f"2D lid-driven cavity {size}x{size}, Re=100"
     else:
-        mesh, model, config, pref = cases.cavity3d(128, iterations=500)
-        desc = "3D lid-driven cavity 128^3 hexahedra, Re=1000"
+        size = size or 128
+        mesh, model, config, pref = cases.cavity3d(size, iterations=500)
+        desc = f"3D lid-driven cavity {size}^3 hexahedra, Re=1000"
     return mesh, model, config, pref, desc
 
 
 # ------------------------------------------------------------ byte model
-def algorithmic_bytes(mesh, kry, ns):
+def algorithmic_bytes(mesh, kry, ns, sk=8):
     """Algorithmic HBM bytes of one SIMPLE iteration given its Krylov counts
-    (U iterations per component, p iterations).  Per-operation figures:
+    (U iterations per component, p iterations); sk is the size of the Krylov
+    iterations' matrix and vector values (8, or 4 in mixed precision).
+    Per-operation figures (s the value size):
       SpMV (CSR, k vectors)   nnz*(s+4) + (N+1)*4 + 2*k*N*s
       DILU apply (k vectors)  2*Fi*(s+4) + 2*N*s + 4*k*N*s
       DILU update             Fi*(2s+4) + 2*N*s
@@ -78,27 +87,28 @@ def algorithmic_bytes(mesh, kry, ns):
     Fi = F - Fb
     nnz = N + 2 * Fi
 
-    def spmv(k):
+    def spmv(k, s=s):
         return nnz * (s + 4) + (N + 1) * 4 + 2 * k * N * s
 
-    def dilu(k):
+    def dilu(k, s=s):
         return 2 * Fi * (s + 4) + 2 * N * s + 4 * k * N * s
     dilu_upd = Fi * (2 * s + 4) + 2 * N * s
     vec = N * s
+    veck = N * sk
     itU = int(max(kry[:ns]))
     itP = int(kry[3])
     b = 0
     # momentum: assembly, r0 = b - A x0, DILU update + first apply, BiCGSTAB init
     b += Fi * (8 + 6 * s) + N * (5 * s + 3 * s * (ns - 1)) + Fb * (4 + 4 * s)
     b += spmv(ns) + dilu_upd + dilu(ns) + 3 * ns * vec
-    b += itU * (2 * spmv(ns) + 2 * dilu(ns) + 20 * ns * vec)
+    b += itU * (2 * spmv(ns, sk) + 2 * dilu(ns, sk) + 20 * ns * veck)
     b += 3 * ns * vec                                    # x + x0
     b += spmv(ns) + (2 + 2) * ns * vec + N * (s + 4)     # residual!, remove_pressure_source!, H!
     b += F * s * (1 + ns) + (1 + ns) * N * s + F * 8     # rDf, Uf(H) face interpolation
     # pressure: div!, assembly, CG
     b += F * s * ns + N * 2 * s + Fi * (8 + 4 * s) + N * 3 * s
     b += spmv(1) + dilu_upd + dilu(1) + 3 * vec
-    b += itP * (spmv(1) + dilu(1) + 13 * vec)
+    b += itP * (spmv(1, sk) + dilu(1, sk) + 13 * veck)
     b += 3 * vec + spmv(1) + 2 * vec                     # relax, residual!
     b += F * s + 2 * N * s                               # pf interpolation
     b += Fi * (8 + 2 * s) + N * s * (1 + ns * 3)         # Green-Gauss + correct_velocity!
@@ -209,9 +219,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    mesh, model, config, pref, desc = build_case(a.config)
+    mesh, model, config, pref, desc = build_case(a.config, a.size)
     N = mesh.ncells
-    workload = f"{a.config}_{N}_fp64_simple"
+    workload = f"{a.config}_{N}_{a.precision}_simple"
 
     if a.impl == "reference":
         if rank != 0:
@@ -241,7 +251,8 @@ def main():
     from xcal import _abi, cases
 
     renum = {"color": _abi.RENUMBER_COLOR, "rcm": _abi.RENUMBER_RCM, "none": _abi.RENUMBER_NONE}[a.renumber]
-    case, keep = X.make_case(model, config, pref)
+    prec = _abi.PREC_MIXED if a.precision == "mixed" else _abi.PREC_FP64
+    case, keep = X.make_case(model, config, pref, prec)
     s = X.Solver(mesh, device=local if world > 1 else 0, renumber=renum)
     s.setup(case)
     U0, p0 = cases.fields(model)
@@ -286,7 +297,8 @@ def main():
     kry = np.array(kry)
     # roofline of the (single) device program kernel
     ns = 3 if mesh.dim == 3 else 2
-    bytes_per_step = np.array([algorithmic_bytes(mesh, kr, ns) for kr in kry], dtype=np.float64)
+    sk = 4 if a.precision == "mixed" else 8
+    bytes_per_step = np.array([algorithmic_bytes(mesh, kr, ns, sk) for kr in kry], dtype=np.float64)
     achieved_gbs = float(bytes_per_step.sum() / (np.array(ms).sum() / 1000.0) / 1e9)
     peak, peak_kind = load_peaks()
 
@@ -327,9 +339,9 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f64+f32",
         "data": "synthetic mesh from the seeded generator (reference UNV construction rules)",
-        "config": {"workload": desc, "cells": N, "renumber": a.renumber,
+        "config": {"workload": desc, "cells": N, "renumber": a.renumber, "precision": a.precision,
                    "step": "one SIMPLE iteration from zero initial fields",
                    "l2": "flushed between steps (256 MiB write)" if flush is not None else "not flushed",
                    "krylov_mean": {"U": float(kry[:, 0].mean()), "p": float(kry[:, 3].mean())},

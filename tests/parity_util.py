@@ -20,8 +20,8 @@ def rel_l2(a, b):
     return num / den if den > 0 else num
 
 
-def run_device(mesh, model, config, pref, iterations, renumber, piso=False):
-    case, keep = X.make_case(model, config, pref)
+def run_device(mesh, model, config, pref, iterations, renumber, piso=False, precision=_abi.PREC_FP64):
+    case, keep = X.make_case(model, config, pref, precision)
     s = X.Solver(mesh, renumber=renumber)
     try:
         s.setup(case)

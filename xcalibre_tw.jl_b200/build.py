@@ -4,7 +4,9 @@
 
 --fmad=false keeps every multiply and add separately rounded, the contract the
 FP64 path's bitwise parity with the CPU oracle depends on (the kernels are
-bandwidth bound, so fused multiply-adds would not make them faster).
+bandwidth bound, so fused multiply-adds would not make them faster).  The
+persistent program (csrc/xcal_kernel.cu) is compiled once per instantiation
+(components x scalar type), in parallel.
 """
 import os
 import subprocess
@@ -15,30 +17,40 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libxcal.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
-         "--expt-relaxed-constexpr"]
-SOURCES = ["xcal_kernel.cu", "xcal_ops.cu", "xcal_api.cu", "host_mesh.cpp"]
+FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "--fmad=false", "-lineinfo",
+         "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "--expt-relaxed-constexpr"]
+INSTANCES = {"d1": (1, "double"), "d2": (2, "double"), "d3": (3, "double"), "f2": (2, "float"),
+             "f3": (3, "float")}
+UNITS = [("xcal_kernel.cu", tag, ["-DXCAL_INST=" + tag, f"-DXCAL_NS={ns}", f"-DXCAL_T={t}"])
+         for tag, (ns, t) in INSTANCES.items()]
+UNITS += [("xcal_launch.cu", None, []), ("xcal_ops.cu", None, []), ("xcal_api.cu", None, []),
+          ("host_mesh.cpp", None, [])]
 
 
 def build(verbose=False):
-    objs = []
     bdir = os.path.join(HERE, "_build")
     os.makedirs(bdir, exist_ok=True)
-    for s in SOURCES:
-        src = os.path.join(CSRC, s)
-        obj = os.path.join(bdir, s + ".o")
-        deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
-        deps.append(os.path.join(HERE, "..", "include", "xcal.h"))
-        if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(d) for d in deps):
-            cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
-            if verbose and s.endswith(".cu"):
-                cmd += ["-Xptxas", "-v"]
-            if s.endswith(".cpp"):
-                cmd = [NVCC] + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
-            subprocess.run(cmd, check=True)
+    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(HERE, "..", "include", "xcal.h"))
+    newest_header = max(os.path.getmtime(h) for h in headers)
+    procs, objs = [], []
+    for src_name, tag, defs in UNITS:
+        src = os.path.join(CSRC, src_name)
+        obj = os.path.join(bdir, src_name + (f".{tag}" if tag else "") + ".o")
         objs.append(obj)
-    cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
-    subprocess.run(cmd, check=True)
+        if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header):
+            continue
+        if src_name.endswith(".cpp"):
+            cmd = [NVCC] + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
+        else:
+            cmd = [NVCC] + ARCH + FLAGS + defs + ["-c", src, "-o", obj]
+            if verbose:
+                cmd += ["-Xptxas", "-v"]
+        procs.append((cmd, subprocess.Popen(cmd)))
+    for cmd, p in procs:
+        if p.wait() != 0:
+            raise RuntimeError("compile failed: " + " ".join(cmd))
+    subprocess.run([NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"], check=True)
     return OUT
 
 

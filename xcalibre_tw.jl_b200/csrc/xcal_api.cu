@@ -414,7 +414,7 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
     if (!(cfg->solver_k.relax > 0.0) || !(cfg->solver_omega.relax > 0.0)) return fail(c, XCAL_ERR_ARG, "relaxation factors must be > 0");
     if (c->ns == 3) return fail(c, XCAL_ERR_UNSUPPORTED, "k-omega is a 2D model in the reference");
   }
-  if (cfg->precision != XCAL_PREC_FP64) return fail(c, XCAL_ERR_UNSUPPORTED, "mixed precision not available");
+  if (cfg->precision != XCAL_PREC_FP64 && cfg->precision != XCAL_PREC_MIXED) return fail(c, XCAL_ERR_ARG, "unknown precision");
   TRY(check_solver(c, cfg->solver_U, "U"));
   TRY(check_solver(c, cfg->solver_p, "p"));
   if (cfg->schemes_U.time == XCAL_TIME_EULER && !(cfg->dt > 0.0)) return fail(c, XCAL_ERR_ARG, "Euler time scheme needs dt > 0");
@@ -463,6 +463,21 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
     for (int b = 0; b < 2; ++b) { w->r[b] = A(m); w->p[b] = A(m); w->v[b] = A(m); }
   }
   h.part = A((size_t)MAXK * h.ntiles);
+  h.prec = cfg->precision;
+  if (h.prec == XCAL_PREC_MIXED) {
+    auto F = [&](size_t cnt) { float *p = B.alloc<float>(cnt); if (!p) ok = false; return p; };
+    for (int k = 0; k < 2; ++k) {
+      MatT<float> &M32 = (k == 0) ? h.AU32 : h.AP32;
+      const Mat &M64 = (k == 0) ? h.AU : h.AP;
+      M32.col = M64.col; M32.tpos = M64.tpos; M32.dpos = M64.dpos; M32.W = M64.W; M32.np = M64.np;
+      M32.precon = M64.precon;
+      M32.val = F(nnz); M32.Dpiv = F(n); M32.Dinv = F(n);
+      KWorkT<float> *w = (k == 0) ? &h.wU32 : &h.wP32;
+      size_t m = (k == 0) ? (size_t)n * NS : (size_t)n;
+      w->x = F(m); w->s = F(m); w->t = F(m); w->q = F(m);
+      for (int b = 0; b < 2; ++b) { w->r[b] = F(m); w->p[b] = F(m); w->v[b] = F(m); }
+    }
+  }
   if (turb) {
     h.k = A(n); h.w = A(n); h.nut = A(n); h.nutf = A(nf); h.nueffk = A(nf); h.nueffw = A(nf);
     h.Dk = A(n); h.Dw = A(n); h.Pk = A(n); h.Pw = A(n); h.G = A((size_t)n * 9);
@@ -573,7 +588,7 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   CUDA_TRY(c, cudaMemsetAsync(h.done, 0, sizeof(int), c->stream));
   h.mode = c->mode;
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-  if (iters > 0) CUDA_TRY(c, launch_program(c->ns, c->mode, c->nblocks, &h, prog, iters, c->stream));
+  if (iters > 0) CUDA_TRY(c, launch_program(c->ns, h.prec == XCAL_PREC_MIXED, c->mode, c->nblocks, &h, prog, iters, c->stream));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   float ms = 0.f;
@@ -739,7 +754,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   }
   h.mode = mode;
   CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
-  CUDA_TRY(c, launch_program(1, mode, nb, &h, PROG_SOLVE, 1, c->stream));
+  CUDA_TRY(c, launch_program(1, 0, mode, nb, &h, PROG_SOLVE, 1, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   Bar bar;
   double so[2];

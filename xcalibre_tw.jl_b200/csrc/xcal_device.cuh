@@ -51,15 +51,18 @@ struct FieldBC {
   const int *fbc;       // [nbf] BC applied to each boundary face by correct_boundaries! (-1: none)
 };
 
-// Sparse matrix in ELL form (shared pattern, own values).
-struct Mat {
+// Sparse matrix in ELL form (shared pattern, own values).  T is the value
+// type: double for the FP64 path, float for the Krylov side of the mixed path.
+template <typename T>
+struct MatT {
   const int *col;       // [W*np]
   const int *tpos;      // [W*np] position of the transposed entry
   const int *dpos;      // [np] position of the diagonal entry
-  double *val;          // [W*np]
-  double *Dpiv, *Dinv;  // DILU pivots and their inverses (or the diagonal scaling)
+  T *val;               // [W*np]
+  T *Dpiv, *Dinv;       // DILU pivots and their inverses (or the diagonal scaling)
   int precon, W, np;
 };
+using Mat = MatT<double>;
 
 struct KCfg {
   int solver, itmax;
@@ -69,9 +72,11 @@ struct KCfg {
 // Krylov vectors, interleaved by system: v[i*NS + s].  p, v and r have two
 // buffers each (the fused phases read the old values of neighbours while
 // writing new ones).
-struct KWork {
-  double *x, *r[2], *p[2], *v[2], *s, *t, *q;
+template <typename T>
+struct KWorkT {
+  T *x, *r[2], *p[2], *v[2], *s, *t, *q;
 };
+using KWork = KWorkT<double>;
 
 struct KParams {
   int n, nf, nbf, dim, ntiles, np, mode, Wf;
@@ -100,6 +105,10 @@ struct KParams {
   KCfg kK, kW;
   int precK, precW, divK, divW, timeK, timeW;
   double aK, aW;
+  // mixed precision: FP32 copies of the matrices and FP32 Krylov vectors
+  int prec;
+  MatT<float> AU32, AP32;
+  KWorkT<float> wU32, wP32;
   // state
   double *U, *Uz2;      // U [n*NS] interleaved; Uz2: z component kept for 2D meshes
   double *p, *gp, *bU, *bP, *H, *rD, *divH;
@@ -243,28 +252,27 @@ __device__ __forceinline__ void final_sum(const double *part, int ntiles, double
 // coalesced); the sums then run in ascending column order.
 struct Row {
   int c[WUNROLL];
-  int W;
 };
-__device__ __forceinline__ void load_row(const Mat &A, int i, Row &r) {
-  r.W = A.W;
+template <typename T>
+__device__ __forceinline__ void load_row(const MatT<T> &A, int i, Row &r) {
 #pragma unroll
   for (int k = 0; k < WUNROLL; ++k) r.c[k] = (k < A.W) ? __ldg(A.col + (size_t)k * A.np + i) : -1;
 }
 
-// y = sum_k val[k]*x[col[k]] in ascending column order from 0.0: the order of
+// y = sum_k val[k]*x[col[k]] in ascending column order from 0: the order of
 // SparseArrays' CSC mul! (column scatter) as seen by one row.  GetX(j, d)
 // returns component d of x at row j (it may compute the value on the fly).
-template <int NS, class GetX>
-__device__ __forceinline__ void spmv_row(const Mat &A, int i, GetX getx, double (&y)[NS]) {
+template <int NS, typename T, class GetX>
+__device__ __forceinline__ void spmv_row(const MatT<T> &A, int i, GetX getx, T (&y)[NS]) {
 #pragma unroll
-  for (int d = 0; d < NS; ++d) y[d] = 0.0;
+  for (int d = 0; d < NS; ++d) y[d] = T(0);
   if (A.W <= WUNROLL) {
     Row r;
     load_row(A, i, r);
 #pragma unroll
     for (int k = 0; k < WUNROLL; ++k) {
       if (r.c[k] >= 0) {
-        const double a = A.val[(size_t)k * A.np + i];
+        const T a = A.val[(size_t)k * A.np + i];
 #pragma unroll
         for (int d = 0; d < NS; ++d) y[d] = y[d] + a * getx(r.c[k], d);
       }
@@ -273,7 +281,7 @@ __device__ __forceinline__ void spmv_row(const Mat &A, int i, GetX getx, double 
     for (int k = 0; k < A.W; ++k) {
       const int j = __ldg(A.col + (size_t)k * A.np + i);
       if (j < 0) continue;
-      const double a = A.val[(size_t)k * A.np + i];
+      const T a = A.val[(size_t)k * A.np + i];
 #pragma unroll
       for (int d = 0; d < NS; ++d) y[d] = y[d] + a * getx(j, d);
     }
@@ -282,36 +290,67 @@ __device__ __forceinline__ void spmv_row(const Mat &A, int i, GetX getx, double 
 
 // DILU pivot of row i (update_dilu_diagonal!, preconditioners_1_DILU.jl:230-251):
 // D_i = A_ii - sum_{j<i} (A_ij*A_ji)/D_j over lower neighbours in ascending j.
-__device__ __forceinline__ void dilu_setup_row(const Mat &A, int i) {
-  double D = A.val[__ldg(A.dpos + i)];
-  for (int k = 0; k < A.W; ++k) {
-    const size_t e = (size_t)k * A.np + i;
-    const int j = __ldg(A.col + e);
-    if (j < 0 || j >= i) break;
-    D = D - A.val[e] * A.val[__ldg(A.tpos + e)] / A.Dpiv[j];
+template <typename T>
+__device__ __forceinline__ void dilu_setup_row(const MatT<T> &A, int i) {
+  T D = A.val[__ldg(A.dpos + i)];
+  if (A.W <= WUNROLL) {
+    // Row entries are in ascending column order, so the lower neighbours are
+    // the entries with 0 <= j < i; all loads are issued before the sums.
+    Row r;
+    load_row(A, i, r);
+#pragma unroll
+    for (int k = 0; k < WUNROLL; ++k) {
+      const int j = r.c[k];
+      if (j >= 0 && j < i) {
+        const size_t e = (size_t)k * A.np + i;
+        D = D - A.val[e] * A.val[__ldg(A.tpos + e)] / A.Dpiv[j];
+      }
+    }
+  } else {
+    for (int k = 0; k < A.W; ++k) {
+      const size_t e = (size_t)k * A.np + i;
+      const int j = __ldg(A.col + e);
+      if (j < 0 || j >= i) break;
+      D = D - A.val[e] * A.val[__ldg(A.tpos + e)] / A.Dpiv[j];
+    }
   }
   A.Dpiv[i] = D;
-  A.Dinv[i] = 1 / D;
+  A.Dinv[i] = T(1) / D;
 }
 
 // Forward row (forward_substitution!, :253-279): o = in_i - sum_{j<i} (A_ij*out_j)*Dinv_j.
 // GetOut(j, d) returns out_j (possibly recomputed); rows without upper
 // neighbours also take the backward step at once (x_i = c_i*Dinv_i).
-template <int NS, class GetOut>
-__device__ __forceinline__ void dilu_fwd_row(const Mat &A, const double (&in)[NS], GetOut geto, int i,
-                                             int blev_i, double (&o)[NS]) {
+template <int NS, typename T, class GetOut>
+__device__ __forceinline__ void dilu_fwd_row(const MatT<T> &A, const T (&in)[NS], GetOut geto, int i,
+                                             int blev_i, T (&o)[NS]) {
 #pragma unroll
   for (int d = 0; d < NS; ++d) o[d] = in[d];
-  for (int k = 0; k < A.W; ++k) {
-    const size_t e = (size_t)k * A.np + i;
-    const int j = __ldg(A.col + e);
-    if (j < 0 || j >= i) break;
-    const double a = A.val[e], dj = A.Dinv[j];
+  if (A.W <= WUNROLL) {
+    Row r;
+    load_row(A, i, r);
 #pragma unroll
-    for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * dj;
+    for (int k = 0; k < WUNROLL; ++k) {
+      const int j = r.c[k];
+      if (j >= 0 && j < i) {
+        const size_t e = (size_t)k * A.np + i;
+        const T a = A.val[e], dj = A.Dinv[j];
+#pragma unroll
+        for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * dj;
+      }
+    }
+  } else {
+    for (int k = 0; k < A.W; ++k) {
+      const size_t e = (size_t)k * A.np + i;
+      const int j = __ldg(A.col + e);
+      if (j < 0 || j >= i) break;
+      const T a = A.val[e], dj = A.Dinv[j];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * dj;
+    }
   }
   if (blev_i == 0) {
-    const double di = A.Dinv[i];
+    const T di = A.Dinv[i];
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = o[d] * di;
   }
@@ -319,37 +358,52 @@ __device__ __forceinline__ void dilu_fwd_row(const Mat &A, const double (&in)[NS
 
 // Backward row (backward_substitution!, :281-308): x_i = c_i*Dinv_i, then
 // x_i -= (A_ij*x_j)*Dinv_i for upper neighbours in ascending j.
-template <int NS>
-__device__ __forceinline__ void dilu_bwd_row(const Mat &A, const double *out, int i, double (&o)[NS]) {
-  const double di = A.Dinv[i];
+template <int NS, typename T>
+__device__ __forceinline__ void dilu_bwd_row(const MatT<T> &A, const T *out, int i, T (&o)[NS]) {
+  const T di = A.Dinv[i];
 #pragma unroll
   for (int d = 0; d < NS; ++d) o[d] = out[(size_t)i * NS + d] * di;
-  for (int k = 0; k < A.W; ++k) {
-    const size_t e = (size_t)k * A.np + i;
-    const int j = __ldg(A.col + e);
-    if (j <= i) continue;
-    const double a = A.val[e];
+  if (A.W <= WUNROLL) {
+    Row r;
+    load_row(A, i, r);
 #pragma unroll
-    for (int d = 0; d < NS; ++d) o[d] = o[d] - a * out[(size_t)j * NS + d] * di;
+    for (int k = 0; k < WUNROLL; ++k) {
+      const int j = r.c[k];
+      if (j > i) {
+        const T a = A.val[(size_t)k * A.np + i];
+#pragma unroll
+        for (int d = 0; d < NS; ++d) o[d] = o[d] - a * out[(size_t)j * NS + d] * di;
+      }
+    }
+  } else {
+    for (int k = 0; k < A.W; ++k) {
+      const size_t e = (size_t)k * A.np + i;
+      const int j = __ldg(A.col + e);
+      if (j <= i) continue;
+      const T a = A.val[e];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) o[d] = o[d] - a * out[(size_t)j * NS + d] * di;
+    }
   }
 }
 
 // Diagonal preconditioners (Jacobi: 1/|A_ii|; NormDiagonal: 1/norm(column i)),
 // preconditioners_2_functions.jl:28-57.
-__device__ __forceinline__ void diag_precon_setup_row(const Mat &A, int i) {
+template <typename T>
+__device__ __forceinline__ void diag_precon_setup_row(const MatT<T> &A, int i) {
   if (A.precon == 1) {
-    A.Dinv[i] = 1 / fabs(A.val[__ldg(A.dpos + i)]);
+    A.Dinv[i] = T(1) / fabs(A.val[__ldg(A.dpos + i)]);
   } else if (A.precon == 2) {
-    double s = 0.0;
+    T s = T(0);
     for (int k = 0; k < A.W; ++k) {
       const size_t e = (size_t)k * A.np + i;
       if (__ldg(A.col + e) < 0) continue;
-      const double a = A.val[__ldg(A.tpos + e)];
+      const T a = A.val[__ldg(A.tpos + e)];
       s += a * a;
     }
-    A.Dinv[i] = 1 / sqrt(s);
+    A.Dinv[i] = T(1) / sqrt(s);
   } else {
-    A.Dinv[i] = 1.0;
+    A.Dinv[i] = T(1);
   }
 }
 

@@ -18,13 +18,33 @@ enum { GRAD_ORTHOGONAL = 0, GRAD_MIDPOINT = 1 };
 enum { SOLVER_CG = 0, SOLVER_BICGSTAB = 1 };
 enum { PRECON_DILU = 0 };
 
+constexpr int MAXTL = 32;   // tiles per CTA whose warp sums are staged in shared memory
+
 struct Ctx {
   const KParams *P;
   Sync S;
   double *sm;       // [8*MAXK]
   double *sm_out;   // [MAXK]
+  double *ws;       // [MAXTL*MAXK*8] staged warp sums
   __device__ bool sync() { return S.sync(); }
 };
+
+template <typename T>
+__device__ __forceinline__ const MatT<T> &matU(const KParams &P) {
+  if constexpr (sizeof(T) == 4) return P.AU32; else return P.AU;
+}
+template <typename T>
+__device__ __forceinline__ const MatT<T> &matP(const KParams &P) {
+  if constexpr (sizeof(T) == 4) return P.AP32; else return P.AP;
+}
+template <typename T>
+__device__ __forceinline__ const KWorkT<T> &workU(const KParams &P) {
+  if constexpr (sizeof(T) == 4) return P.wU32; else return P.wU;
+}
+template <typename T>
+__device__ __forceinline__ const KWorkT<T> &workP(const KParams &P) {
+  if constexpr (sizeof(T) == 4) return P.wP32; else return P.wP;
+}
 
 // ---------------------------------------------------------------- phases
 template <class F>
@@ -36,22 +56,50 @@ __device__ __forceinline__ void tile_each(const KParams &P, F f) {
 }
 
 // One row per thread per tile; with `reduce`, the K values returned by f are
-// summed per tile with the canonical tree into part[k*ntiles + t].
+// summed per tile with the canonical tree into part[k*ntiles + t].  The warp
+// stage of each tile's tree runs as the rows finish and is staged in shared
+// memory; the 8-way stage of all the CTA's tiles runs once at the end, so the
+// warps are not held at a block barrier per tile.
 template <int K, class F>
 __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
   const KParams &P = *C.P;
-  for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-    const int i = t * TILE + threadIdx.x;
-    double v[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = 0.0;
-    if (i < P.n) f(i, v);
-    if (reduce) {
-      block_tree<K>(v, C.sm);
-      if (threadIdx.x == 0)
-#pragma unroll
-        for (int k = 0; k < K; ++k) P.part[(size_t)k * P.ntiles + t] = v[k];
+  const int G = gridDim.x, nt = P.ntiles;
+  if (!reduce) {
+    for (int t = blockIdx.x; t < nt; t += G) {
+      const int i = t * TILE + threadIdx.x;
+      double v[K];
+      if (i < P.n) f(i, v);
     }
+    return;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int t0 = blockIdx.x; t0 < nt; t0 += MAXTL * G) {   // chunks of at most MAXTL tiles
+    int tl = 0;
+    for (int t = t0; t < nt && tl < MAXTL; t += G, ++tl) {
+      const int i = t * TILE + threadIdx.x;
+      double v[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) v[k] = 0.0;
+      if (i < P.n) f(i, v);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) v[k] = v[k] + __shfl_down_sync(0xffffffffu, v[k], off);
+        if (lane == 0) C.ws[(tl * K + k) * 8 + wid] = v[k];
+      }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < tl * K; q += TPB) {
+      const double *w = C.ws + q * 8;
+      double a0 = w[0] + w[4], a1 = w[1] + w[5];
+      const double a2 = w[2] + w[6], a3 = w[3] + w[7];
+      a0 = a0 + a2;
+      a1 = a1 + a3;
+      a0 = a0 + a1;
+      const int k = q % K, t = t0 + (q / K) * G;
+      P.part[(size_t)k * nt + t] = a0;
+    }
+    __syncthreads();
   }
 }
 
@@ -75,21 +123,21 @@ __device__ __forceinline__ void st(double *a, int i, const double (&o)[NS]) {
 // Row-local part of M^{-1}: DILU forward level 0 (and the backward step of
 // rows without upper neighbours) or a diagonal scaling.  Returns false when
 // the row has no row-local part (DILU rows of level >= 1).
-template <int NS>
-__device__ __forceinline__ bool precon_local(const KParams &P, const Mat &A, int i, const double (&in)[NS],
-                                             double (&o)[NS]) {
+template <int NS, typename T>
+__device__ __forceinline__ bool precon_local(const KParams &P, const MatT<T> &A, int i, const T (&in)[NS],
+                                             T (&o)[NS]) {
   if (A.precon == PRECON_DILU) {
     if (__ldg(P.flev + i) != 0) return false;
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = in[d];
     if (__ldg(P.blev + i) == 0) {
-      const double di = A.Dinv[i];
+      const T di = A.Dinv[i];
 #pragma unroll
       for (int d = 0; d < NS; ++d) o[d] = o[d] * di;
     }
     return true;
   }
-  const double di = A.Dinv[i];
+  const T di = A.Dinv[i];
 #pragma unroll
   for (int d = 0; d < NS; ++d) o[d] = di * in[d];
   return true;
@@ -97,7 +145,8 @@ __device__ __forceinline__ bool precon_local(const KParams &P, const Mat &A, int
 
 // Number of phases of M^{-1} after its producer phase.  The producer did the
 // row-local part (and, with first_lvl == 2, forward level 1 as well).
-__device__ __forceinline__ int precon_tail_phases(const KParams &P, const Mat &A, bool setup, int first_lvl) {
+template <typename T>
+__device__ __forceinline__ int precon_tail_phases(const KParams &P, const MatT<T> &A, bool setup, int first_lvl) {
   if (A.precon != PRECON_DILU) return setup ? 1 : 0;
   return max(0, P.nfl - first_lvl) + (P.nbl - 1);
 }
@@ -105,9 +154,8 @@ __device__ __forceinline__ int precon_tail_phases(const KParams &P, const Mat &A
 // The remaining phases of M^{-1} (in -> out).  With `setup` the DILU pivots
 // (update_preconditioner!) are computed level by level in the same phases.
 // The last phase also computes the K partial sums red(i, v).
-template <int NS, int K, class Red>
-__device__ bool precon_tail(Ctx &C, const Mat &A, const double *in, double *out, bool setup, int first_lvl,
-                            Red red) {
+template <int NS, int K, typename T, class Red>
+__device__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *in, T *out, bool setup, int first_lvl, Red red) {
   const KParams &P = *C.P;
   const int nph = precon_tail_phases(P, A, setup, first_lvl);
   if (nph == 0 && setup) {   // nothing left to apply: reduce in a phase of its own
@@ -118,7 +166,7 @@ __device__ bool precon_tail(Ctx &C, const Mat &A, const double *in, double *out,
     if (!setup) return true;
     tile_phase<K>(C, true, [&](int i, double (&v)[K]) {
       diag_precon_setup_row(A, i);
-      const double di = A.Dinv[i];
+      const T di = A.Dinv[i];
 #pragma unroll
       for (int d = 0; d < NS; ++d) out[(size_t)i * NS + d] = di * in[(size_t)i * NS + d];
       red(i, v);
@@ -131,10 +179,12 @@ __device__ bool precon_tail(Ctx &C, const Mat &A, const double *in, double *out,
     tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
       if (__ldg(P.flev + i) == l) {
         if (setup) dilu_setup_row(A, i);
-        double iv[NS], o[NS];
-        ld<NS>(in, i, iv);
+        T iv[NS], o[NS];
+#pragma unroll
+        for (int d = 0; d < NS; ++d) iv[d] = in[(size_t)i * NS + d];
         dilu_fwd_row<NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, __ldg(P.blev + i), o);
-        st<NS>(out, i, o);
+#pragma unroll
+        for (int d = 0; d < NS; ++d) out[(size_t)i * NS + d] = o[d];
       }
       if (last) red(i, v);
     });
@@ -144,9 +194,10 @@ __device__ bool precon_tail(Ctx &C, const Mat &A, const double *in, double *out,
     const bool last = (++ph == nph);
     tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
       if (__ldg(P.blev + i) == l) {
-        double o[NS];
+        T o[NS];
         dilu_bwd_row<NS>(A, out, i, o);
-        st<NS>(out, i, o);
+#pragma unroll
+        for (int d = 0; d < NS; ++d) out[(size_t)i * NS + d] = o[d];
       }
       if (last) red(i, v);
     });
@@ -155,41 +206,59 @@ __device__ bool precon_tail(Ctx &C, const Mat &A, const double *in, double *out,
   return true;
 }
 
-// Krylov start for row i (Krylov.jl warm start): r0 = b - A*x0 over the row
-// just assembled, x = 0, the DILU pivot of level-0 rows and the row-local part
-// of the first M^{-1}.  BiCGSTAB keeps r0 in q and preconditions into r[0];
-// CG keeps r[0] = r0 and preconditions into v[0].
-template <int NS>
-__device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A, const KWork &w,
-                                                const double (&b)[NS], const double *x0, int i, int solver) {
-  double y[NS], r0[NS];
-  spmv_row<NS>(A, i, [&](int j, int d) { return x0[(size_t)j * NS + d]; }, y);
+// Krylov start for row i (Krylov.jl warm start): r0 = b - A*x0 in FP64 over
+// the row just assembled, x = 0, the DILU pivot of level-0 rows and the
+// row-local part of the first M^{-1}.  With T = float the row is also copied
+// to the FP32 matrix the Krylov iterations use (iterative refinement: the
+// FP64 residual r0 is the right-hand side of an FP32 correction solve).
+// BiCGSTAB keeps r0 in q and preconditions into r[0]; CG keeps r[0] = r0 and
+// preconditions into v[0].
+template <int NS, typename T>
+__device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A64, const MatT<T> &A,
+                                                const KWorkT<T> &w, const double (&b)[NS], const double *x0,
+                                                int i, int solver) {
+  if constexpr (sizeof(T) == 4) {
+    for (int k = 0; k < A.W; ++k) {
+      const size_t e = (size_t)k * A.np + i;
+      if (__ldg(A.col + e) >= 0) A.val[e] = (float)A64.val[e];
+    }
+  }
+  double y[NS];
+  T r0[NS];
+  spmv_row<NS>(A64, i, [&](int j, int d) { return x0[(size_t)j * NS + d]; }, y);
 #pragma unroll
   for (int d = 0; d < NS; ++d) {
-    r0[d] = b[d] - y[d];
-    w.x[(size_t)i * NS + d] = 0.0;
+    r0[d] = (T)(b[d] - y[d]);
+    w.x[(size_t)i * NS + d] = T(0);
   }
   if (A.precon == PRECON_DILU && __ldg(P.flev + i) == 0) dilu_setup_row(A, i);
-  double o[NS];
+  T o[NS];
   const bool dilu = (A.precon == PRECON_DILU);
   if (solver == SOLVER_BICGSTAB) {
-    st<NS>(w.q, i, r0);
-    if (dilu && precon_local<NS>(P, A, i, r0, o)) st<NS>(w.r[0], i, o);
+#pragma unroll
+    for (int d = 0; d < NS; ++d) w.q[(size_t)i * NS + d] = r0[d];
+    if (dilu && precon_local<NS>(P, A, i, r0, o))
+#pragma unroll
+      for (int d = 0; d < NS; ++d) w.r[0][(size_t)i * NS + d] = o[d];
   } else {
-    st<NS>(w.r[0], i, r0);
-    if (dilu && precon_local<NS>(P, A, i, r0, o)) st<NS>(w.v[0], i, o);
+#pragma unroll
+    for (int d = 0; d < NS; ++d) w.r[0][(size_t)i * NS + d] = r0[d];
+    if (dilu && precon_local<NS>(P, A, i, r0, o))
+#pragma unroll
+      for (int d = 0; d < NS; ++d) w.v[0][(size_t)i * NS + d] = o[d];
   }
 }
 
 // Set-up phases of M and its first application after the assembly phase,
-// with the initial dot products (CG: <r,z>; BiCGSTAB: <b,r>, <r,r>).
-template <int NS>
-__device__ bool krylov_start(Ctx &C, const Mat &A, const KWork &w, const double *b, int solver) {
+// with the initial dot products (CG: <r,z>; BiCGSTAB: <b,r>, <r,r>), all
+// accumulated in FP64.
+template <int NS, typename T>
+__device__ bool krylov_start(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, int solver) {
   if (solver == SOLVER_BICGSTAB) {
     return precon_tail<NS, 2 * NS>(C, A, w.q, w.r[0], true, 1, [&](int i, double (&v)[2 * NS]) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
-        const double rv = w.r[0][(size_t)i * NS + d];
+        const double rv = (double)w.r[0][(size_t)i * NS + d];
         v[2 * d] = b[(size_t)i * NS + d] * rv;
         v[2 * d + 1] = rv * rv;
       }
@@ -197,7 +266,8 @@ __device__ bool krylov_start(Ctx &C, const Mat &A, const KWork &w, const double 
   }
   return precon_tail<NS, NS>(C, A, w.r[0], w.v[0], true, 1, [&](int i, double (&v)[NS]) {
 #pragma unroll
-    for (int d = 0; d < NS; ++d) v[d] = w.r[0][(size_t)i * NS + d] * w.v[0][(size_t)i * NS + d];
+    for (int d = 0; d < NS; ++d)
+      v[d] = (double)w.r[0][(size_t)i * NS + d] * (double)w.v[0][(size_t)i * NS + d];
   });
 }
 
@@ -210,8 +280,9 @@ __device__ bool krylov_start(Ctx &C, const Mat &A, const KWork &w, const double 
 //   D  s = r - alpha*v (recomputed for neighbours), x += alpha*p, q = A s, M^-1 level 0
 //   .. remaining M^-1 phases, last one reduces <t,s>, <t,t>
 //   G  x += omega*s, r = s - omega*t, reduces <b,r>, <r,r>
-template <int NS>
-__device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb, const KCfg &cfg,
+// Vector updates are evaluated in FP64 and stored in T; dots accumulate in FP64.
+template <int NS, typename T>
+__device__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *bb, const KCfg &cfg,
                          int (&its)[NS], double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   double red[2 * NS];
@@ -231,7 +302,7 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
     const bool solved = rnorm[d] <= eps[d], tired = 0 >= cfg.itmax;
     if (!(solved || tired)) active |= 1u << d;
   }
-  double *r = w.r[0];
+  T *r = w.r[0];
   const int tail = precon_tail_phases(P, A, false, 1);
   int pc = 0;
   bool first = true;
@@ -239,32 +310,35 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
 #pragma unroll
     for (int d = 0; d < NS; ++d)
       if (active & (1u << d)) { its[d] += 1; rho[d] = nrho[d]; }
-    double *pn = w.p[pc], *po = w.p[pc ^ 1], *vn = w.v[pc], *vo = w.v[pc ^ 1];
-    auto getp = [&](int j, int d) -> double {
+    T *pn = w.p[pc], *po = w.p[pc ^ 1], *vn = w.v[pc], *vo = w.v[pc ^ 1];
+    auto getp = [&](int j, int d) -> T {
       const size_t k = (size_t)j * NS + d;
       if (first) return r[k];
-      const double pv = po[k] + (-omega[d]) * vo[k];
-      return r[k] + beta[d] * pv;
+      const double pv = (double)po[k] + (-omega[d]) * (double)vo[k];
+      return (T)((double)r[k] + beta[d] * pv);
     };
     // A: p update, q = A p, M^{-1} row-local part
     tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
-      double y[NS], pi[NS], o[NS];
+      T y[NS], pi[NS], o[NS];
       spmv_row<NS>(A, i, getp, y);
 #pragma unroll
       for (int d = 0; d < NS; ++d) pi[d] = getp(i, d);
 #pragma unroll
       for (int d = 0; d < NS; ++d)
         if (active & (1u << d)) pn[(size_t)i * NS + d] = pi[d];
-      st<NS>(w.q, i, y);
-      if (precon_local<NS>(P, A, i, y, o)) st<NS>(vn, i, o);
+#pragma unroll
+      for (int d = 0; d < NS; ++d) w.q[(size_t)i * NS + d] = y[d];
+      if (precon_local<NS>(P, A, i, y, o))
+#pragma unroll
+        for (int d = 0; d < NS; ++d) vn[(size_t)i * NS + d] = o[d];
       if (tail == 0)
 #pragma unroll
-        for (int d = 0; d < NS; ++d) v[d] = bb[(size_t)i * NS + d] * o[d];
+        for (int d = 0; d < NS; ++d) v[d] = bb[(size_t)i * NS + d] * (double)o[d];
     });
     if (!C.sync()) return false;
-    if (!precon_tail<NS, NS>(C, A, w.q, vn, false, 1, [&](int i, double (&v)[NS]) {
+    if (!precon_tail<NS, NS>(C, A, (const T *)w.q, vn, false, 1, [&](int i, double (&v)[NS]) {
 #pragma unroll
-          for (int d = 0; d < NS; ++d) v[d] = bb[(size_t)i * NS + d] * vn[(size_t)i * NS + d];
+          for (int d = 0; d < NS; ++d) v[d] = bb[(size_t)i * NS + d] * (double)vn[(size_t)i * NS + d];
         }))
       return false;
     {
@@ -274,36 +348,42 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
       for (int d = 0; d < NS; ++d)
         if (active & (1u << d)) alpha[d] = rho[d] / cv[d];
     }
-    auto gets = [&](int j, int d) -> double {
+    auto gets = [&](int j, int d) -> T {
       const size_t k = (size_t)j * NS + d;
-      return r[k] + (-alpha[d]) * vn[k];
+      return (T)((double)r[k] + (-alpha[d]) * (double)vn[k]);
     };
     // D: s, x += alpha p, q = A s, M^{-1} row-local part
     tile_phase<2 * NS>(C, tail == 0, [&](int i, double (&v)[2 * NS]) {
-      double y[NS], o[NS], si[NS];
+      T y[NS], o[NS], si[NS];
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
         si[d] = gets(i, d);
         if (active & (1u << d)) {
           w.s[k] = si[d];
-          w.x[k] = w.x[k] + alpha[d] * pn[k];
+          w.x[k] = (T)((double)w.x[k] + alpha[d] * (double)pn[k]);
         }
       }
       spmv_row<NS>(A, i, gets, y);
-      st<NS>(w.q, i, y);
-      if (precon_local<NS>(P, A, i, y, o)) st<NS>(w.t, i, o);
+#pragma unroll
+      for (int d = 0; d < NS; ++d) w.q[(size_t)i * NS + d] = y[d];
+      if (precon_local<NS>(P, A, i, y, o))
+#pragma unroll
+        for (int d = 0; d < NS; ++d) w.t[(size_t)i * NS + d] = o[d];
       if (tail == 0)
 #pragma unroll
-        for (int d = 0; d < NS; ++d) { v[2 * d] = o[d] * si[d]; v[2 * d + 1] = o[d] * o[d]; }
+        for (int d = 0; d < NS; ++d) {
+          v[2 * d] = (double)o[d] * (double)si[d];
+          v[2 * d + 1] = (double)o[d] * (double)o[d];
+        }
     });
     if (!C.sync()) return false;
-    if (!precon_tail<NS, 2 * NS>(C, A, w.q, w.t, false, 1, [&](int i, double (&v)[2 * NS]) {
+    if (!precon_tail<NS, 2 * NS>(C, A, (const T *)w.q, w.t, false, 1, [&](int i, double (&v)[2 * NS]) {
 #pragma unroll
           for (int d = 0; d < NS; ++d) {
             const size_t k = (size_t)i * NS + d;
-            const double tv = w.t[k];
-            v[2 * d] = tv * w.s[k];
+            const double tv = (double)w.t[k];
+            v[2 * d] = tv * (double)w.s[k];
             v[2 * d + 1] = tv * tv;
           }
         }))
@@ -317,12 +397,13 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
-        double rv = r[k];
+        double rv = (double)r[k];
         if (active & (1u << d)) {
-          const double sv = w.s[k];
-          w.x[k] = w.x[k] + omega[d] * sv;
-          rv = sv + (-omega[d]) * w.t[k];
-          r[k] = rv;
+          const double sv = (double)w.s[k];
+          w.x[k] = (T)((double)w.x[k] + omega[d] * sv);
+          const T rt = (T)(sv + (-omega[d]) * (double)w.t[k]);
+          r[k] = rt;
+          rv = (double)rt;
         }
         v[2 * d] = bb[k] * rv;
         v[2 * d + 1] = rv * rv;
@@ -362,8 +443,8 @@ __device__ bool bicgstab(Ctx &C, const Mat &A, const KWork &w, const double *bb,
 //   B  x += alpha p, r -= alpha q, M^-1 levels 0 and 1 (level-0 values of
 //      neighbours recomputed), backward step of rows without upper neighbours
 //   .. remaining M^-1 phases, the last reduces <r,z>
-template <int NS>
-__device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&its)[NS],
+template <int NS, typename T>
+__device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg, int (&its)[NS],
                    double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   const double EPS = 2.220446049250313e-16;
@@ -383,31 +464,31 @@ __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&
     const bool solved = rnorm[d] <= eps[d], tired = 0 >= cfg.itmax;
     if (!(solved || tired)) active |= 1u << d;
   }
-  const double *z = w.v[0];
-  double *zw = w.v[0];
+  const T *z = w.v[0];
+  T *zw = w.v[0];
   const bool dilu = (A.precon == PRECON_DILU);
   const bool lvl1 = dilu && P.nfl >= 2;
   const int tail = dilu ? precon_tail_phases(P, A, false, 2) : 0;
   int rc = 0, pc = 0;
   bool first = true;
   while (active) {
-    double *pn = w.p[pc], *po = w.p[pc ^ 1];
-    auto getp = [&](int j, int d) -> double {
+    T *pn = w.p[pc], *po = w.p[pc ^ 1];
+    auto getp = [&](int j, int d) -> T {
       const size_t k = (size_t)j * NS + d;
       if (first) return z[k];
-      return z[k] + beta[d] * po[k];
+      return (T)((double)z[k] + beta[d] * (double)po[k]);
     };
     // A: p update, q = A p, <p,q>
     tile_phase<NS>(C, true, [&](int i, double (&v)[NS]) {
-      double y[NS];
+      T y[NS];
       spmv_row<NS>(A, i, getp, y);
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
-        const double pi = getp(i, d);
+        const T pi = getp(i, d);
         if (active & (1u << d)) pn[(size_t)i * NS + d] = pi;
-        v[d] = pi * y[d];
+        v[d] = (double)pi * (double)y[d];
+        w.q[(size_t)i * NS + d] = y[d];
       }
-      st<NS>(w.q, i, y);
     });
     if (!C.sync()) return false;
     final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
@@ -422,20 +503,20 @@ __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&
     }
     active = upd;
     if (!active) break;
-    double *ro = w.r[rc], *rn = w.r[rc ^ 1];
-    auto getr = [&](int j, int d) -> double {
+    T *ro = w.r[rc], *rn = w.r[rc ^ 1];
+    auto getr = [&](int j, int d) -> T {
       const size_t k = (size_t)j * NS + d;
-      return ro[k] + (-alpha[d]) * w.q[k];
+      return (T)((double)ro[k] + (-alpha[d]) * (double)w.q[k]);
     };
     // B: x, r updates and M^{-1} levels 0/1
     tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
-      double rr[NS], o[NS];
+      T rr[NS], o[NS];
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
         rr[d] = getr(i, d);
         if (active & (1u << d)) {
-          w.x[k] = w.x[k] + alpha[d] * pn[k];
+          w.x[k] = (T)((double)w.x[k] + alpha[d] * (double)pn[k]);
           rn[k] = rr[d];
         }
       }
@@ -444,15 +525,17 @@ __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&
         dilu_fwd_row<NS>(A, rr, getr, i, __ldg(P.blev + i), o);
         have = true;
       }
-      if (have) st<NS>(zw, i, o);
+      if (have)
+#pragma unroll
+        for (int d = 0; d < NS; ++d) zw[(size_t)i * NS + d] = o[d];
       if (tail == 0)
 #pragma unroll
-        for (int d = 0; d < NS; ++d) v[d] = rr[d] * o[d];
+        for (int d = 0; d < NS; ++d) v[d] = (double)rr[d] * (double)o[d];
     });
     if (!C.sync()) return false;
-    if (dilu && !precon_tail<NS, NS>(C, A, rn, zw, false, 2, [&](int i, double (&v)[NS]) {
+    if (dilu && !precon_tail<NS, NS>(C, A, (const T *)rn, zw, false, 2, [&](int i, double (&v)[NS]) {
 #pragma unroll
-          for (int d = 0; d < NS; ++d) v[d] = rn[(size_t)i * NS + d] * z[(size_t)i * NS + d];
+          for (int d = 0; d < NS; ++d) v[d] = (double)rn[(size_t)i * NS + d] * (double)z[(size_t)i * NS + d];
         }))
       return false;
     final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
@@ -483,11 +566,11 @@ __device__ bool cg(Ctx &C, const Mat &A, const KWork &w, const KCfg &cfg, int (&
   return true;
 }
 
-template <int NS>
-__device__ bool krylov(Ctx &C, const Mat &A, const KWork &w, const double *b, const KCfg &cfg,
+template <int NS, typename T>
+__device__ bool krylov(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, const KCfg &cfg,
                        int solver, int (&its)[NS], double (&rn)[NS]) {
-  if (solver == SOLVER_BICGSTAB) return bicgstab<NS>(C, A, w, b, cfg, its, rn);
-  return cg<NS>(C, A, w, cfg, its, rn);
+  if (solver == SOLVER_BICGSTAB) return bicgstab<NS, T>(C, A, w, b, cfg, its, rn);
+  return cg<NS, T>(C, A, w, cfg, its, rn);
 }
 
 // -------------------------------------------------------------- assembly
@@ -968,7 +1051,7 @@ __device__ __forceinline__ void bound_row(const KParams &P, double *fld, int i) 
   fld[i] = jmax(jmax(fi, average * (signbit(fi) ? 1.0 : 0.0)), EPS);
 }
 
-template <int NS>
+template <int NS, typename T>
 __device__ bool turbulence(Ctx &C) {
   const KParams &P = *C.P;
   const double nu = P.nu;
@@ -1020,27 +1103,28 @@ __device__ bool turbulence(Ctx &C) {
     P.nueffk[f] = nu + KW_SIGK * P.nutf[f];
   });
   if (!C.sync()) return false;
+  const KWorkT<T> &wk = workP<T>(P);
   for (int eq = 0; eq < 2; ++eq) {   // omega first, then k
     const bool om = (eq == 0);
-    Mat A = P.AP;
+    MatT<T> A = matP<T>(P);
     A.precon = om ? P.precW : P.precK;
     double *phi = om ? P.w : P.k;
     const KCfg &cfg = om ? P.kW : P.kK;
     tile_each(P, [&](int i) {
       double b[1];
-      b[0] = om ? scalar_row(P, A, i, phi, P.nueffw, P.Dw, P.Pw, P.bcW, P.aW, P.divW, P.timeW, true)
-                : scalar_row(P, A, i, phi, P.nueffk, P.Dk, P.Pk, P.bcK, P.aK, P.divK, P.timeK, false);
+      b[0] = om ? scalar_row(P, P.AP, i, phi, P.nueffw, P.Dw, P.Pw, P.bcW, P.aW, P.divW, P.timeW, true)
+                : scalar_row(P, P.AP, i, phi, P.nueffk, P.Dk, P.Pk, P.bcK, P.aK, P.divK, P.timeK, false);
       P.bP[i] = b[0];
-      krylov_init_row<1>(P, A, P.wP, b, phi, i, cfg.solver);
+      krylov_init_row<1, T>(P, P.AP, A, wk, b, phi, i, cfg.solver);
     });
     if (!C.sync()) return false;
-    if (!krylov_start<1>(C, A, P.wP, P.bP, cfg.solver)) return false;
+    if (!krylov_start<1, T>(C, A, wk, P.bP, cfg.solver)) return false;
     int its[1];
     double rn[1];
-    if (!krylov<1>(C, A, P.wP, P.bP, cfg, cfg.solver, its, rn)) return false;
+    if (!krylov<1, T>(C, A, wk, P.bP, cfg, cfg.solver, its, rn)) return false;
     // run! copy-back, then constrain_boundary! for omega (:401-448)
     tile_each(P, [&](int i) {
-      double v = P.wP.x[i] + phi[i];
+      double v = (double)wk.x[i] + phi[i];
       if (om) {
         const FieldBC &bc = P.bcW;
         for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
@@ -1082,7 +1166,7 @@ __device__ bool turbulence(Ctx &C) {
 }
 
 // ------------------------------------------------------------- programs
-template <int NS>
+template <int NS, typename T>
 __device__ void simple_program(Ctx &C, int iters, bool piso) {
   const KParams &P = *C.P;
   const bool mid = (P.grad == GRAD_MIDPOINT);
@@ -1101,22 +1185,24 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     done = it + 1;
     double Rit[4] = {1.0, 1.0, 1.0, 1.0};
     // ---- momentum: assemble, start Krylov, set up M, solve
+    const MatT<T> &AUT = matU<T>(P);
+    const KWorkT<T> &wU = workU<T>(P);
     tile_each(P, [&](int i) {
       double b[NS];
       momentum_row<NS>(P, i, !piso, b);
-      krylov_init_row<NS>(P, P.AU, P.wU, b, P.U, i, P.kU.solver);
+      krylov_init_row<NS, T>(P, P.AU, AUT, wU, b, P.U, i, P.kU.solver);
     });
     if (!C.sync()) return;
-    if (!krylov_start<NS>(C, P.AU, P.wU, P.bU, P.kU.solver)) return;
+    if (!krylov_start<NS, T>(C, AUT, wU, P.bU, P.kU.solver)) return;
     int itsU[NS];
     double rnU[NS];
-    if (!krylov<NS>(C, P.AU, P.wU, P.bU, P.kU, P.kU.solver, itsU, rnU)) return;
+    if (!krylov<NS, T>(C, AUT, wU, P.bU, P.kU, P.kU.solver, itsU, rnU)) return;
     // run! copy-back: U = x + x0
     tile_each(P, [&](int i) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
-        P.U[k] = P.wU.x[k] + P.U[k];
+        P.U[k] = (double)wU.x[k] + P.U[k];
       }
     });
     if (!C.sync()) return;
@@ -1172,19 +1258,21 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       });
       if (!C.sync()) return;
       // div! + pressure assembly + Krylov start
+      const MatT<T> &APT = matP<T>(P);
+      const KWorkT<T> &wP = workP<T>(P);
       tile_each(P, [&](int i) {
         double b[1];
         b[0] = pressure_row<NS>(P, i);
-        krylov_init_row<1>(P, P.AP, P.wP, b, P.p, i, P.kP.solver);
+        krylov_init_row<1, T>(P, P.AP, APT, wP, b, P.p, i, P.kP.solver);
       });
       if (!C.sync()) return;
-      if (!krylov_start<1>(C, P.AP, P.wP, P.bP, P.kP.solver)) return;
+      if (!krylov_start<1, T>(C, APT, wP, P.bP, P.kP.solver)) return;
       int itsP[1];
       double rnP[1];
-      if (!krylov<1>(C, P.AP, P.wP, P.bP, P.kP, P.kP.solver, itsP, rnP)) return;
+      if (!krylov<1, T>(C, APT, wP, P.bP, P.kP, P.kP.solver, itsP, rnP)) return;
       // run! copy-back then explicit_relaxation!(p, prev, alpha_p)
       tile_each(P, [&](int i) {
-        const double pn = P.wP.x[i] + P.p[i];
+        const double pn = (double)wP.x[i] + P.p[i];
         const double p0 = P.p[i];
         P.p[i] = p0 + P.aP * (pn - p0);
       });
@@ -1213,7 +1301,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       // interpolate!(Uf, U) + correct_boundaries! + flux!(mdotf, Uf)
       grid_each(P.nf, [&](int f) { face_mdot<NS>(P, f); });
       if (!C.sync()) return;
-      if (P.model == 1 && !turbulence<NS>(C)) return;
+      if (P.model == 1 && !turbulence<NS, T>(C)) return;
     }
     if (!piso) {
       // convergence test (Solvers_1_SIMPLE.jl:200-215); every CTA holds the
@@ -1233,10 +1321,10 @@ __device__ void solve_program(Ctx &C) {
   const KParams &P = *C.P;
   tile_each(P, [&](int i) {
     double b[1] = {P.sb[i]};
-    krylov_init_row<1>(P, P.AU, P.wU, b, P.U, i, P.solve_solver);
+    krylov_init_row<1, double>(P, P.AU, P.AU, P.wU, b, P.U, i, P.solve_solver);
   });
   if (!C.sync()) return;
-  if (!krylov_start<1>(C, P.AU, P.wU, P.sb, P.solve_solver)) return;
+  if (!krylov_start<1, double>(C, P.AU, P.wU, P.sb, P.solve_solver)) return;
   KCfg cfg;
   cfg.solver = P.solve_solver;
   cfg.itmax = P.solve_itmax;
@@ -1244,7 +1332,7 @@ __device__ void solve_program(Ctx &C) {
   cfg.rtol = P.solve_rtol;
   int its[1];
   double rn[1];
-  if (!krylov<1>(C, P.AU, P.wU, P.sb, cfg, P.solve_solver, its, rn)) return;
+  if (!krylov<1, double>(C, P.AU, P.wU, P.sb, cfg, P.solve_solver, its, rn)) return;
   tile_each(P, [&](int i) { P.U[i] = P.wU.x[i] + P.U[i]; });
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     P.solve_out[0] = (double)its[0];
@@ -1256,11 +1344,13 @@ __device__ void solve_program(Ctx &C) {
 }  // namespace
 
 // KParams is passed by value: the fields live in the kernel's constant
-// parameter bank instead of occupying registers.
-template <int NS>
+// parameter bank instead of occupying registers.  T is the scalar type of
+// the Krylov iterations (double: FP64 path; float: mixed path).
+template <int NS, typename T>
 __global__ void __launch_bounds__(TPB, 2) xcal_program_kernel(const __grid_constant__ KParams prm, int prog, int iters) {
   __shared__ double sm[8 * MAXK];
   __shared__ double sm_out[MAXK];
+  __shared__ double ws[MAXTL * MAXK * 8];
   __shared__ int sm_ok;
   Ctx C;
   C.P = &prm;
@@ -1271,77 +1361,21 @@ __global__ void __launch_bounds__(TPB, 2) xcal_program_kernel(const __grid_const
   C.S.ok = &sm_ok;
   C.sm = sm;
   C.sm_out = sm_out;
+  C.ws = ws;
   if (prog == PROG_SOLVE) {
-    if (NS == 1) solve_program(C);
+    if constexpr (NS == 1 && sizeof(T) == 8) solve_program(C);
     return;
   }
-  simple_program<NS>(C, iters, prog == PROG_PISO);
+  if constexpr (NS >= 2) simple_program<NS, T>(C, iters, prog == PROG_PISO);
 }
 
-template __global__ void xcal_program_kernel<1>(const __grid_constant__ KParams, int, int);
-template __global__ void xcal_program_kernel<2>(const __grid_constant__ KParams, int, int);
-template __global__ void xcal_program_kernel<3>(const __grid_constant__ KParams, int, int);
-
-// ------------------------------------------------------------ host launch
-const void *program_kernel_ptr(int ns) {
-  if (ns == 1) return (const void *)xcal_program_kernel<1>;
-  if (ns == 2) return (const void *)xcal_program_kernel<2>;
-  return (const void *)xcal_program_kernel<3>;
-}
-
-cudaError_t launch_program(int ns, int mode, int nblocks, const KParams *hparams, int prog, int iters,
-                           cudaStream_t stream) {
-  const void *fn = program_kernel_ptr(ns);
-  void *args[3];
-  args[0] = (void *)hparams;
-  args[1] = (void *)&prog;
-  args[2] = (void *)&iters;
-  if (mode == SYNC_BLOCK) return cudaLaunchKernel(fn, dim3(1), dim3(TPB), args, 0, stream);
-  if (mode == SYNC_CLUSTER) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return e;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nblocks);
-    cfg.blockDim = dim3(TPB);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = nblocks;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, fn, args);
-  }
-  return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(TPB), args, 0, stream);
-}
-
-int max_coresident_blocks(int ns, int device) {
-  int per_sm = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, program_kernel_ptr(ns), TPB, 0);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return per_sm * sms;
-}
-
-int max_cluster_blocks(int ns) {
-  const void *fn = program_kernel_ptr(ns);
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 8;
-  for (int c = 16; c >= 1; c >>= 1) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c);
-    cfg.blockDim = dim3(TPB);
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = c;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) == cudaSuccess && nclusters >= 1) return c;
-  }
-  return 1;
-}
+// One translation unit per instantiation (build.py compiles this file once per
+// XCAL_INST value, in parallel); the launcher table lives in xcal_launch.cu.
+#if defined(XCAL_INST)
+#define XCAL_CAT2(a, b) a##b
+#define XCAL_CAT(a, b) XCAL_CAT2(a, b)
+template __global__ void xcal_program_kernel<XCAL_NS, XCAL_T>(const __grid_constant__ KParams, int, int);
+const void *XCAL_CAT(program_kernel_, XCAL_INST)() { return (const void *)xcal_program_kernel<XCAL_NS, XCAL_T>; }
+#endif
 
 }  // namespace xcal

@@ -5,9 +5,9 @@
 #include "xcal_device.cuh"
 
 namespace xcal {
-cudaError_t launch_program(int ns, int mode, int nblocks, const KParams *hparams, int prog, int iters,
+cudaError_t launch_program(int ns, int mixed, int mode, int nblocks, const KParams *hparams, int prog, int iters,
                            cudaStream_t stream);
 int max_coresident_blocks(int ns, int device);
 int max_cluster_blocks(int ns);
-const void *program_kernel_ptr(int ns);
+const void *program_kernel_ptr(int ns, int mixed);
 }  // namespace xcal
