@@ -30,6 +30,7 @@ extern "C" {
 
 /* ---------------------------------------------------------------- status */
 enum {
+  XCAL_PENDING = 1,          /* xcal_serve_poll: the case has not finished yet */
   XCAL_OK = 0,
   XCAL_ERR_ARG = -1,         /* invalid argument or size */
   XCAL_ERR_MESH = -2,        /* inconsistent or corrupt mesh */
@@ -68,7 +69,10 @@ enum { XCAL_PREC_FP64 = 0, XCAL_PREC_MIXED = 1 };
 enum { XCAL_FIELD_UX = 0, XCAL_FIELD_UY = 1, XCAL_FIELD_UZ = 2, XCAL_FIELD_P = 3,
        XCAL_FIELD_K = 4, XCAL_FIELD_OMEGA = 5, XCAL_FIELD_NUT = 6 };
 /* context flags */
-enum { XCAL_FLAG_ABORT_ON_NAN = 1u, XCAL_FLAG_PHASE_TIMERS = 2u };
+/* XCAL_FLAG_CLUSTER: run every program as one hardware thread-block cluster
+ * (at most 16 CTAs, hardware cluster barrier), the launch form that is safe
+ * to overlap with other contexts' runs on the same GPU (the serving loop). */
+enum { XCAL_FLAG_ABORT_ON_NAN = 1u, XCAL_FLAG_PHASE_TIMERS = 2u, XCAL_FLAG_CLUSTER = 4u };
 
 /* ----------------------------------------------------------------- mesh */
 /*
@@ -137,6 +141,10 @@ typedef struct xcal_ctx_s *xcal_ctx;
 int xcal_ctx_create(int device, uint32_t flags, xcal_ctx *out);
 int xcal_ctx_destroy(xcal_ctx ctx);
 int xcal_last_error(xcal_ctx ctx, char *buf, size_t n);
+/* SIMPLE stop tolerance: a run stops once R_ux, R_uy (R_uz) and R_p are all
+ * <= tol.  The reference hard-codes 1e-7 (src/Solvers/Solvers_1_SIMPLE.jl:200-215),
+ * which is the default; the serving loop uses 1e-6. */
+int xcal_ctx_set_tolerance(xcal_ctx ctx, double tol);
 int xcal_version(int *major, int *minor);
 
 /* Mesh construction on the host (replaces build_mesh + update_mesh_format,
@@ -236,6 +244,53 @@ int xcal_residual(xcal_ctx ctx, int64_t n, const int32_t *row_ptr, const int32_t
  * context's stream; calls that overlap on the GPU share the array and race. */
 int xcal_residual_noalloc(xcal_ctx ctx, int64_t n, const int32_t *d_row_ptr, const int32_t *d_col,
                           const double *d_val, const double *d_x, const double *d_b, double *d_R);
+
+/* ------------------------------------------------------------- serving
+ * A stream of independent cases on one GPU (no reference counterpart: the
+ * reference solves one case per process).  Each submitted case is copied
+ * (mesh, case, initial fields), then set up and run by one of `slots` worker
+ * threads, each owning a context created with XCAL_FLAG_CLUSTER, so up to
+ * `slots` cases run concurrently as separate hardware clusters.  A case runs
+ * until every residual is <= tolerance or max_iterations.  The caller's
+ * arrays are not referenced after xcal_serve_submit returns. */
+typedef struct xcal_server_s *xcal_server;
+typedef struct {
+  int32_t slots;            /* concurrent cases (worker threads), 1..64 */
+  int32_t max_iterations;   /* per-case SIMPLE iteration cap */
+  int32_t renumber;         /* XCAL_RENUMBER_* for every case */
+  int32_t pad;
+  double tolerance;         /* stop when all residuals <= tolerance */
+} xcal_serve_cfg;
+typedef struct {
+  int32_t status;           /* XCAL_OK or the failing call's status */
+  int32_t iterations;       /* SIMPLE iterations run */
+  int32_t converged;        /* 1 when the tolerance was reached */
+  int32_t ncells;
+  double residual[4];       /* last R_ux, R_uy, R_uz, R_p */
+  double queue_ms;          /* submit -> a worker picked the case up */
+  double setup_ms;          /* mesh upload, renumbering, case set-up, fields */
+  double run_ms;            /* device time of the SIMPLE run */
+  double total_ms;          /* submit -> result ready */
+} xcal_serve_result;
+typedef struct {
+  int64_t submitted, completed, failed, queued, running;
+  double cell_iterations;   /* sum over finished cases of cells x iterations */
+  double run_ms;            /* sum of device run times */
+} xcal_serve_stats;
+int xcal_serve_create(int device, const xcal_serve_cfg *cfg, xcal_server *out);
+/* U0 holds ux, uy, uz (3 x ncells, the caller's cell order); p0 ncells.
+ * Either may be NULL (zero initial field).  *ticket identifies the case. */
+int xcal_serve_submit(xcal_server s, const xcal_mesh_desc *mesh, const xcal_case *cfg,
+                      const double *U0, const double *p0, int64_t *ticket);
+/* wait_ms: 0 = do not wait, < 0 = wait until done.  Returns XCAL_PENDING while
+ * the case runs; once done, fills *res and (when non-NULL) U (3 x ncells) and
+ * p (ncells), releases the case and returns XCAL_OK (res->status carries a
+ * failed case's error). */
+int xcal_serve_poll(xcal_server s, int64_t ticket, int32_t wait_ms, xcal_serve_result *res,
+                    double *U, double *p);
+int xcal_serve_stats_get(xcal_server s, xcal_serve_stats *st);
+/* Finishes the running cases, drops the queued ones, joins the workers. */
+int xcal_serve_destroy(xcal_server s);
 
 #ifdef __cplusplus
 }

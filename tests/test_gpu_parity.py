@@ -85,6 +85,22 @@ def test_barrier_modes_identical(sync, monkeypatch):
     assert np.array_equal(dev["U"], ref["U"])
 
 
+@pytest.mark.parametrize("fuse", ["0", "1"], ids=["cg3", "cg2"])
+def test_cg_fused_and_split_phases(fuse, monkeypatch):
+    """CG with the two-level DILU applied inside the x/r phase (2 grid
+    barriers per iteration) and with a separate backward phase (3 barriers):
+    both agree bitwise with the oracle, on 2D and 3D meshes."""
+    monkeypatch.setenv("XCAL_CG_FUSE", fuse)
+    mesh, model, config, pref = cases.bfs(6, iterations=40)
+    dev = run_device(mesh, model, config, pref, 40, _abi.RENUMBER_COLOR)
+    orc = run_oracle(dev["dev_mesh"], model, config, pref, 40, dev["perm"])
+    assert_parity(dev, orc)
+    mesh, model, config, pref = cases.cavity3d(10, iterations=15)
+    dev = run_device(mesh, model, config, pref, 15, _abi.RENUMBER_COLOR)
+    orc = run_oracle(dev["dev_mesh"], model, config, pref, 15, dev["perm"])
+    assert_parity(dev, orc, nU=3)
+
+
 def _snapshot_matrix(n=24, iters=5):
     mesh, model, config, pref = cases.cavity2d(n, iterations=iters)
     om = O.from_mesh2(mesh)

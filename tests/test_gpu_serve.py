@@ -1,0 +1,103 @@
+"""Serving loop (xcal_serve_*): a stream of independent cases run concurrently
+on one GPU, each as one hardware cluster on its worker's stream.
+
+A case's result inside the mix must equal its result run alone through the
+plain path (one context, same precision, same stop tolerance): the device
+program's arithmetic does not depend on the launch form or on other work on
+the GPU, so the comparison is bitwise (iteration count, residual history end,
+fields).  Mixed-precision results are also compared with the FP64 plain path
+(relative L2, reported)."""
+import numpy as np
+import pytest
+
+import xcal as X
+from xcal import _abi, cases
+from parity_util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6
+MAXIT = 3000
+
+
+def _alone(c, precision):
+    case, keep = X.make_case(c["model"], c["config"], c["pref"], precision)
+    s = X.Solver(c["mesh"], renumber=_abi.RENUMBER_COLOR)
+    try:
+        s.setup(case)
+        s.set_tolerance(TOL)
+        U, p = cases.fields(c["model"])
+        for f, v in ((_abi.FIELD_UX, U[0]), (_abi.FIELD_UY, U[1]), (_abi.FIELD_UZ, U[2]), (_abi.FIELD_P, p)):
+            s.set_field(f, v)
+        out = s.run(MAXIT, want_krylov=False)
+        out["U"] = np.stack([s.get_field(_abi.FIELD_UX), s.get_field(_abi.FIELD_UY), s.get_field(_abi.FIELD_UZ)])
+        out["p"] = s.get_field(_abi.FIELD_P)
+    finally:
+        s.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_serve_matches_alone(precision):
+    # Re <= 60: the reference SIMPLE (upwind, no Rhie-Chow, relax 0.7/0.3)
+    # diverges on the coarse BFS meshes from about Re 125 (the CPU oracle
+    # does the same), and those cases are covered by the divergence test.
+    stream = cases.serving_stream(6, rate=1000.0, seed=7, nmin=16, nmax=48, re_max=60.0)
+    srv = X.Server(slots=4, max_iterations=MAXIT, tolerance=TOL)
+    try:
+        tickets = [srv.submit(c["model"], c["config"], c["pref"], precision) for c in stream]
+        results = [srv.poll(t, wait_ms=-1) for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(stream) and st["failed"] == 0
+    for c, r in zip(stream, results):
+        assert r["status"] == 0
+        a = _alone(c, precision)
+        assert r["iterations"] == a["done"], (c["kind"], c["N"], r["iterations"], a["done"])
+        assert r["converged"] == 1 and a["done"] < MAXIT
+        last = a["done"] - 1
+        assert r["residual"][0] == a["R_ux"][last] and r["residual"][3] == a["R_p"][last]
+        assert np.array_equal(r["U"], a["U"]) and np.array_equal(r["p"], a["p"])
+        if precision == _abi.PREC_MIXED:
+            f = _alone(c, _abi.PREC_FP64)
+            d = max(rel_l2(r["U"][0], f["U"][0]), rel_l2(r["U"][1], f["U"][1]))
+            print(c["kind"], c["N"], round(c["Re"]), "mixed vs fp64 U rel L2", d, r["iterations"], f["done"])
+            assert d <= 1e-3
+
+
+def test_serve_stats_and_errors():
+    srv = X.Server(slots=2, max_iterations=50, tolerance=TOL)
+    try:
+        c = cases.serving_stream(1, seed=3, nmin=16, nmax=16, re_max=60.0)[0]
+        t = srv.submit(c["model"], c["config"], c["pref"])
+        r = srv.poll(t, wait_ms=-1)
+        assert r["status"] == 0 and r["iterations"] <= 50
+        with pytest.raises(_abi.XcalError):
+            srv.poll(t)                  # a ticket is released once its result was read
+        st = srv.stats()
+        assert st["submitted"] == 1 and st["completed"] == 1 and st["queued"] == 0 and st["running"] == 0
+        assert st["cell_iterations"] == c["mesh"].ncells * r["iterations"]
+    finally:
+        srv.close()
+
+
+def test_serve_stops_a_diverged_case():
+    """A case whose residuals become non-finite is stopped at that iteration
+    (XCAL_FLAG_ABORT_ON_NAN on the serving contexts) and reported with status
+    XCAL_ERR_NAN; the other cases are unaffected."""
+    stream = cases.serving_stream(2, rate=1000.0, seed=11, nmin=16, nmax=24, re_max=60.0)
+    bad = stream[0]
+    bad["model"].p.values[3] = np.nan
+    srv = X.Server(slots=2, max_iterations=500, tolerance=TOL)
+    try:
+        tb = srv.submit(bad["model"], bad["config"], bad["pref"])
+        tg = srv.submit(stream[1]["model"], stream[1]["config"], stream[1]["pref"])
+        rb = srv.poll(tb, wait_ms=-1)
+        rg = srv.poll(tg, wait_ms=-1)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert rb["status"] == -5 and rb["iterations"] == 1
+    assert rg["status"] == 0 and rg["converged"] == 1
+    assert st["failed"] == 1 and st["completed"] == 1

@@ -39,6 +39,19 @@ def test_ctx_create_without_device_fails_cleanly():
     assert _abi.load().xcal_ctx_create(0, 0, C.byref(h)) == -4   # XCAL_ERR_CUDA
 
 
+def test_serve_config_validation():
+    """xcal_serve_create checks its configuration before touching a device."""
+    lib = _abi.load()
+    h = C.c_void_p()
+    for bad in (dict(slots=0), dict(slots=65), dict(max_iterations=0), dict(tolerance=-1.0),
+                dict(renumber=7)):
+        cfg = dict(slots=2, max_iterations=10, renumber=2, pad=0, tolerance=1e-6)
+        cfg.update(bad)
+        assert lib.xcal_serve_create(0, C.byref(_abi.ServeCfg(**cfg)), C.byref(h)) == -1, bad
+    assert lib.xcal_serve_poll(None, 1, 0, None, None, None) == -1
+    assert lib.xcal_ctx_set_tolerance(None, 1e-6) == -1
+
+
 def _has_gpu():
     try:
         import torch

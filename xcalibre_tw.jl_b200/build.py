@@ -18,13 +18,13 @@ OUT = os.path.join(HERE, "libxcal.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "--fmad=false", "-lineinfo",
-         "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "--expt-relaxed-constexpr"]
+         "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "--expt-relaxed-constexpr", "-diag-suppress=177"]
 INSTANCES = {"d1": (1, "double"), "d2": (2, "double"), "d3": (3, "double"), "f2": (2, "float"),
              "f3": (3, "float")}
 UNITS = [("xcal_kernel.cu", tag, ["-DXCAL_INST=" + tag, f"-DXCAL_NS={ns}", f"-DXCAL_T={t}"])
          for tag, (ns, t) in INSTANCES.items()]
 UNITS += [("xcal_launch.cu", None, []), ("xcal_ops.cu", None, []), ("xcal_api.cu", None, []),
-          ("host_mesh.cpp", None, [])]
+          ("host_mesh.cpp", None, []), ("xcal_serve.cpp", None, [])]
 
 
 def build(verbose=False):
@@ -50,7 +50,7 @@ def build(verbose=False):
     for cmd, p in procs:
         if p.wait() != 0:
             raise RuntimeError("compile failed: " + " ".join(cmd))
-    subprocess.run([NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"], check=True)
+    subprocess.run([NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart", "-lpthread"], check=True)
     return OUT
 
 

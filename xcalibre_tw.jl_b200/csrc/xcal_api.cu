@@ -20,19 +20,23 @@ using namespace xcal;
 
 namespace {
 
-// Device allocations of one context, released together.
+// Device allocations of one context, released together.  They are ordered
+// on the context's stream (cudaMallocAsync/cudaFreeAsync): a plain cudaFree
+// would synchronise the whole device and stall the runs of other contexts
+// (the serving loop keeps several in flight on one GPU).
 struct DevBuf {
   std::vector<void *> ptrs;
+  cudaStream_t stream = nullptr;
   ~DevBuf() { release(); }
   void release() {
-    for (void *p : ptrs) cudaFree(p);
+    for (void *p : ptrs) cudaFreeAsync(p, stream);
     ptrs.clear();
   }
   template <class T>
   T *alloc(size_t n) {
     if (n == 0) n = 1;
     void *p = nullptr;
-    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    if (cudaMallocAsync(&p, n * sizeof(T), stream) != cudaSuccess) return nullptr;
     ptrs.push_back(p);
     return (T *)p;
   }
@@ -54,7 +58,7 @@ struct xcal_ctx_s {
   int mode = SYNC_GRID, nblocks = 1;
   DevBuf mbuf, cbuf, rbuf;     // mesh, case, run buffers
   KParams hp;
-  KParams *dp = nullptr;
+  double conv = 1e-7;          // SIMPLE stop tolerance
   int run_cap = 0;
   double last_ms = 0.0;
   double *pin = nullptr;       // pinned staging [n*3]
@@ -76,11 +80,30 @@ static int fail(xcal_ctx c, int code, const std::string &msg) {
     if (e_ != cudaSuccess) return fail(c, XCAL_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// Blocking copy on the context's stream (the stream-ordered allocations are
+// only ordered with that stream).
+static cudaError_t copy_sync(xcal_ctx c, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, c->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(c->stream);
+}
+
+// Zero a device range with a copy-engine transfer rather than a memset
+// kernel: a memset kernel would have to wait for a free SM while other
+// contexts' persistent programs occupy the GPU (serving), a copy does not.
+// A pageable source is staged before cudaMemcpyAsync returns, so the zero
+// buffer may be reused at once.
+static cudaError_t zero_dev(xcal_ctx c, void *dst, size_t bytes) {
+  static thread_local std::vector<char> zeros;
+  if (zeros.size() < bytes) zeros.assign(bytes, 0);
+  return cudaMemcpyAsync(dst, zeros.data(), bytes, cudaMemcpyHostToDevice, c->stream);
+}
+
 template <class T>
 static int upload(xcal_ctx c, DevBuf &buf, T *&dst, const std::vector<T> &src) {
   dst = buf.alloc<T>(src.size());
   if (!dst) return fail(c, XCAL_ERR_OOM, "device allocation failed");
-  if (!src.empty()) CUDA_TRY(c, cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!src.empty()) CUDA_TRY(c, copy_sync(c, dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
   return XCAL_OK;
 }
 template <class T>
@@ -96,13 +119,35 @@ static int upload_c(xcal_ctx c, DevBuf &buf, const T *&dst, const std::vector<T>
     if (s_ != XCAL_OK) return s_; \
   } while (0)
 
-static void choose_launch(xcal_ctx c, int n) {
+// CG with a two-level DILU can apply M^{-1} inside its x/r phase by
+// recomputing neighbour values (2 instead of 3 grid barriers per iteration,
+// identical results).  On B200 the extra chain of dependent L2 gathers costs
+// more than the barrier it saves (47,385-cell BFS: 1.73 vs 1.48 ms per SIMPLE
+// iteration; 128^3 cavity: 44 vs 33 ms), so it is off unless XCAL_CG_FUSE=1.
+static int choose_cg_fuse(int ntiles, int nblocks) {
+  const char *f = getenv("XCAL_CG_FUSE");
+  (void)ntiles; (void)nblocks;
+  return f ? atoi(f) != 0 : 0;
+}
+
+static void choose_launch_mode(xcal_ctx c, int n);
+static void choose_launch(xcal_ctx c, int n, KParams &h) {
+  choose_launch_mode(c, n);
+  h.cg_fuse = choose_cg_fuse((n + TILE - 1) / TILE, c->nblocks);
+}
+
+static void choose_launch_mode(xcal_ctx c, int n) {
   int ntiles = (n + TILE - 1) / TILE;
   const char *m = getenv("XCAL_SYNC");
   const char *nbv = getenv("XCAL_NBLOCKS");
   int ns = c->ns;
   int maxco = max_coresident_blocks(ns, c->device);
   if (m && !strcmp(m, "block")) { c->mode = SYNC_BLOCK; c->nblocks = 1; return; }
+  if ((c->flags & XCAL_FLAG_CLUSTER) && !m) {   // one hardware cluster: safe beside other kernels
+    c->mode = SYNC_CLUSTER;
+    c->nblocks = std::max(1, std::min(max_cluster_blocks(ns), ntiles));
+    return;
+  }
   if (m && !strcmp(m, "cluster")) {
     c->mode = SYNC_CLUSTER;
     int mc = max_cluster_blocks(ns);
@@ -149,6 +194,15 @@ int xcal_ctx_create(int device, uint32_t flags, xcal_ctx *out) {
     delete c;
     return XCAL_ERR_CUDA;
   }
+  c->mbuf.stream = c->cbuf.stream = c->rbuf.stream = c->stream;
+  // Keep freed stream-ordered memory in the device's pool: with the default
+  // release threshold (0) every synchronisation would hand it back and the
+  // next set-up would map fresh memory again.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   *out = c;
   return XCAL_OK;
 }
@@ -165,6 +219,13 @@ int xcal_ctx_destroy(xcal_ctx c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+  return XCAL_OK;
+}
+
+int xcal_ctx_set_tolerance(xcal_ctx c, double tol) {
+  if (!c) return XCAL_ERR_ARG;
+  if (!(tol >= 0.0)) return fail(c, XCAL_ERR_ARG, "tolerance must be >= 0");
+  c->conv = tol;
   return XCAL_OK;
 }
 
@@ -309,7 +370,7 @@ int xcal_mesh_upload(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
   const int *ecol, *etpos, *edpos;
   TRY(upload_c(c, B, ecol, P.e_col)); TRY(upload_c(c, B, etpos, P.e_tpos)); TRY(upload_c(c, B, edpos, P.dpos));
   for (Mat *A : {&h.AU, &h.AP}) { A->col = ecol; A->tpos = etpos; A->dpos = edpos; A->W = P.W; A->np = P.np; }
-  choose_launch(c, P.n);
+  choose_launch(c, P.n, h);
   c->have_mesh = true;
   return XCAL_OK;
 }
@@ -486,24 +547,20 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   h.done = B.alloc<int>(1);
   if (!ok || !h.bar || !h.done) return fail(c, XCAL_ERR_OOM, "device allocation failed");
   if (turb) {
-    CUDA_TRY(c, cudaMemsetAsync(h.k, 0, sizeof(double) * n, c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(h.w, 0, sizeof(double) * n, c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(h.nut, 0, sizeof(double) * n, c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(h.nutf, 0, sizeof(double) * nf, c->stream));
+    CUDA_TRY(c, zero_dev(c, h.k, sizeof(double) * n));
+    CUDA_TRY(c, zero_dev(c, h.w, sizeof(double) * n));
+    CUDA_TRY(c, zero_dev(c, h.nut, sizeof(double) * n));
+    CUDA_TRY(c, zero_dev(c, h.nutf, sizeof(double) * nf));
   }
   // fields start at zero (ScalarField/VectorField constructors)
-  CUDA_TRY(c, cudaMemsetAsync(h.U, 0, sizeof(double) * n * NS, c->stream));
-  CUDA_TRY(c, cudaMemsetAsync(h.Uz2, 0, sizeof(double) * n, c->stream));
-  CUDA_TRY(c, cudaMemsetAsync(h.p, 0, sizeof(double) * n, c->stream));
-  CUDA_TRY(c, cudaMemsetAsync(h.gp, 0, sizeof(double) * n * NS, c->stream));
-  CUDA_TRY(c, cudaMemsetAsync(h.AU.val, 0, sizeof(double) * nnz, c->stream));
-  CUDA_TRY(c, cudaMemsetAsync(h.AP.val, 0, sizeof(double) * nnz, c->stream));
-  CUDA_TRY(c, cudaMemsetAsync(h.bU, 0, sizeof(double) * n * NS, c->stream));
-  CUDA_TRY(c, cudaMemsetAsync(h.bP, 0, sizeof(double) * n, c->stream));
-  if (!c->dp) {
-    c->dp = c->mbuf.alloc<KParams>(1);
-    if (!c->dp) return fail(c, XCAL_ERR_OOM, "device allocation failed");
-  }
+  CUDA_TRY(c, zero_dev(c, h.U, sizeof(double) * n * NS));
+  CUDA_TRY(c, zero_dev(c, h.Uz2, sizeof(double) * n));
+  CUDA_TRY(c, zero_dev(c, h.p, sizeof(double) * n));
+  CUDA_TRY(c, zero_dev(c, h.gp, sizeof(double) * n * NS));
+  CUDA_TRY(c, zero_dev(c, h.AU.val, sizeof(double) * nnz));
+  CUDA_TRY(c, zero_dev(c, h.AP.val, sizeof(double) * nnz));
+  CUDA_TRY(c, zero_dev(c, h.bU, sizeof(double) * n * NS));
+  CUDA_TRY(c, zero_dev(c, h.bP, sizeof(double) * n));
   if (!c->pin || c->pin_n < (size_t)n * 3) {
     if (c->pin) cudaFreeHost(c->pin);
     c->pin = nullptr;
@@ -587,6 +644,8 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
   CUDA_TRY(c, cudaMemsetAsync(h.done, 0, sizeof(int), c->stream));
   h.mode = c->mode;
+  h.conv = c->conv;
+  h.abort_nan = (c->flags & XCAL_FLAG_ABORT_ON_NAN) ? 1 : 0;
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
   if (iters > 0) CUDA_TRY(c, launch_program(c->ns, h.prec == XCAL_PREC_MIXED, c->mode, c->nblocks, &h, prog, iters, c->stream));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
@@ -596,13 +655,13 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   c->last_ms = ms;
   Bar bar;
   int dn = 0;
-  CUDA_TRY(c, cudaMemcpy(&bar, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost));
-  CUDA_TRY(c, cudaMemcpy(&dn, h.done, sizeof(int), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy_sync(c, &bar, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy_sync(c, &dn, h.done, sizeof(int), cudaMemcpyDeviceToHost));
   std::vector<double> R((size_t)std::max(iters, 1) * 4);
   std::vector<int> K((size_t)std::max(iters, 1) * 5);
   if (iters > 0) {
-    CUDA_TRY(c, cudaMemcpy(R.data(), h.R, sizeof(double) * iters * 4, cudaMemcpyDeviceToHost));
-    CUDA_TRY(c, cudaMemcpy(K.data(), h.kry, sizeof(int) * iters * 5, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, copy_sync(c, R.data(), h.R, sizeof(double) * iters * 4, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, copy_sync(c, K.data(), h.kry, sizeof(int) * iters * 5, cudaMemcpyDeviceToHost));
   }
   for (int i = 0; i < iters; ++i) {
     if (Rux) Rux[i] = R[4 * i];
@@ -613,6 +672,8 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   if (kry) std::copy(K.begin(), K.begin() + (size_t)iters * 5, kry);
   if (done) *done = dn;
   if (bar.err) return fail(c, XCAL_ERR_TIMEOUT, "device barrier timed out");
+  if (bar.nonfinite)
+    return fail(c, XCAL_ERR_NAN, "non-finite residual at iteration " + std::to_string(dn) + "; run stopped");
   return XCAL_OK;
 }
 
@@ -642,14 +703,14 @@ int xcal_equation_get(xcal_ctx c, int32_t which, double *vals, double *b0, doubl
   size_t ne = (size_t)c->prep.W * c->prep.np;
   std::vector<double> ell(ne);
   auto to_csr = [&](const double *dev) -> int {
-    CUDA_TRY(c, cudaMemcpy(ell.data(), dev, sizeof(double) * ne, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, copy_sync(c, ell.data(), dev, sizeof(double) * ne, cudaMemcpyDeviceToHost));
     for (int k = 0; k < nnz; ++k) vals[k] = ell[c->prep.csr2ell[k]];
     return XCAL_OK;
   };
   if (which == 0) {
     if (vals) TRY(to_csr(h.AU.val));
     std::vector<double> b((size_t)n * NS);
-    CUDA_TRY(c, cudaMemcpy(b.data(), h.bU, sizeof(double) * n * NS, cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, copy_sync(c, b.data(), h.bU, sizeof(double) * n * NS, cudaMemcpyDeviceToHost));
     double *dst[3] = {b0, b1, b2};
     for (int d = 0; d < NS; ++d)
       if (dst[d]) for (int i = 0; i < n; ++i) dst[d][i] = b[(size_t)i * NS + d];
@@ -657,7 +718,7 @@ int xcal_equation_get(xcal_ctx c, int32_t which, double *vals, double *b0, doubl
   }
   if (which == 1) {
     if (vals) TRY(to_csr(h.AP.val));
-    if (b0) CUDA_TRY(c, cudaMemcpy(b0, h.bP, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (b0) CUDA_TRY(c, copy_sync(c, b0, h.bP, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return XCAL_OK;
   }
   return fail(c, XCAL_ERR_ARG, "which must be 0 (momentum) or 1 (pressure)");
@@ -719,6 +780,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   fl.resize(np, 0);
   bl.resize(np, 0);
   DevBuf B;
+  B.stream = c->stream;
   KParams h;
   memset(&h, 0, sizeof(h));
   h.n = n; h.ntiles = np / TILE; h.np = np;
@@ -748,7 +810,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   {
     int saved_ns = c->ns, saved_mode = c->mode, saved_nb = c->nblocks;
     c->ns = 1;
-    choose_launch(c, n);
+    choose_launch(c, n, h);
     mode = c->mode; nb = c->nblocks;
     c->ns = saved_ns; c->mode = saved_mode; c->nblocks = saved_nb;
   }
@@ -758,9 +820,9 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   Bar bar;
   double so[2];
-  CUDA_TRY(c, cudaMemcpy(&bar, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost));
-  CUDA_TRY(c, cudaMemcpy(so, h.solve_out, sizeof(so), cudaMemcpyDeviceToHost));
-  CUDA_TRY(c, cudaMemcpy(x, h.U, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy_sync(c, &bar, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy_sync(c, so, h.solve_out, sizeof(so), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy_sync(c, x, h.U, sizeof(double) * n, cudaMemcpyDeviceToHost));
   if (niter) *niter = (int32_t)so[0];
   if (final_rnorm) *final_rnorm = so[1];
   if (bar.err) return fail(c, XCAL_ERR_TIMEOUT, "device barrier timed out");
@@ -789,6 +851,7 @@ int xcal_residual(xcal_ctx c, int64_t n64, const int32_t *row_ptr, const int32_t
   int nnz = row_ptr[n];
   int ntiles = (n + TILE - 1) / TILE;
   DevBuf B;
+  B.stream = c->stream;
   std::vector<int> rp(row_ptr, row_ptr + n + 1), cl(col, col + nnz);
   std::vector<double> vv(val, val + nnz), xx(x, x + n), bb(b, b + n);
   int *drp, *dcl;

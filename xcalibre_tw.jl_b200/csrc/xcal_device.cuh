@@ -31,7 +31,7 @@ enum { ST_OK = 0, ST_TIMEOUT = 1 };
 struct Bar {
   unsigned long long count;
   int err;
-  int pad;
+  int nonfinite;   // set when a run stopped on a non-finite residual
 };
 
 struct BcEntry {
@@ -90,6 +90,9 @@ struct KParams {
   const int *cb_ptr, *cb_face;
   const int *flev, *blev;                 // [np]
   int nfl, nbl;
+  int cg_fuse;
+  int abort_nan;   // stop at the first non-finite residual
+  double conv;   // SIMPLE stop: every residual <= conv (1e-7 in the reference)   // CG: M^{-1} of a two-level DILU inside the x/r phase (2 barriers per iteration)
   Mat AU, AP;
   FieldBC bcU, bcP;
   // configuration
@@ -358,11 +361,12 @@ __device__ __forceinline__ void dilu_fwd_row(const MatT<T> &A, const T (&in)[NS]
 
 // Backward row (backward_substitution!, :281-308): x_i = c_i*Dinv_i, then
 // x_i -= (A_ij*x_j)*Dinv_i for upper neighbours in ascending j.
-template <int NS, typename T>
-__device__ __forceinline__ void dilu_bwd_row(const MatT<T> &A, const T *out, int i, T (&o)[NS]) {
+template <int NS, typename T, class GetOut>
+__device__ __forceinline__ void dilu_bwd_row_g(const MatT<T> &A, const T (&out_i)[NS], GetOut geto, int i,
+                                               T (&o)[NS]) {
   const T di = A.Dinv[i];
 #pragma unroll
-  for (int d = 0; d < NS; ++d) o[d] = out[(size_t)i * NS + d] * di;
+  for (int d = 0; d < NS; ++d) o[d] = out_i[d] * di;
   if (A.W <= WUNROLL) {
     Row r;
     load_row(A, i, r);
@@ -372,7 +376,7 @@ __device__ __forceinline__ void dilu_bwd_row(const MatT<T> &A, const T *out, int
       if (j > i) {
         const T a = A.val[(size_t)k * A.np + i];
 #pragma unroll
-        for (int d = 0; d < NS; ++d) o[d] = o[d] - a * out[(size_t)j * NS + d] * di;
+        for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * di;
       }
     }
   } else {
@@ -382,9 +386,17 @@ __device__ __forceinline__ void dilu_bwd_row(const MatT<T> &A, const T *out, int
       if (j <= i) continue;
       const T a = A.val[e];
 #pragma unroll
-      for (int d = 0; d < NS; ++d) o[d] = o[d] - a * out[(size_t)j * NS + d] * di;
+      for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * di;
     }
   }
+}
+
+template <int NS, typename T>
+__device__ __forceinline__ void dilu_bwd_row(const MatT<T> &A, const T *out, int i, T (&o)[NS]) {
+  T oi[NS];
+#pragma unroll
+  for (int d = 0; d < NS; ++d) oi[d] = out[(size_t)i * NS + d];
+  dilu_bwd_row_g<NS>(A, oi, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, o);
 }
 
 // Diagonal preconditioners (Jacobi: 1/|A_ii|; NormDiagonal: 1/norm(column i)),

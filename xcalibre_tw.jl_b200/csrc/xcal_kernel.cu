@@ -468,7 +468,13 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
   T *zw = w.v[0];
   const bool dilu = (A.precon == PRECON_DILU);
   const bool lvl1 = dilu && P.nfl >= 2;
-  const int tail = dilu ? precon_tail_phases(P, A, false, 2) : 0;
+  // With two forward levels every level-1 row has only lower neighbours and
+  // every level-0 row only upper ones, so the whole of M^{-1} r fits in the
+  // x/r phase: level-0 rows recompute their upper neighbours' forward values
+  // (which in turn recompute r of their level-0 neighbours).  Same row
+  // functions, same inputs: identical bits, one grid barrier fewer.
+  const bool fuse = dilu && P.nfl == 2 && P.cg_fuse;
+  const int tail = (dilu && !fuse) ? precon_tail_phases(P, A, false, 2) : 0;
   int rc = 0, pc = 0;
   bool first = true;
   while (active) {
@@ -520,10 +526,29 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
           rn[k] = rr[d];
         }
       }
-      bool have = precon_local<NS>(P, A, i, rr, o);
-      if (!have && lvl1 && __ldg(P.flev + i) == 1) {
-        dilu_fwd_row<NS>(A, rr, getr, i, __ldg(P.blev + i), o);
+      bool have;
+      if (fuse) {
+        if (__ldg(P.flev + i) == 1) {
+          dilu_fwd_row<NS>(A, rr, getr, i, 0, o);
+        } else if (__ldg(P.blev + i) == 0) {
+#pragma unroll
+          for (int d = 0; d < NS; ++d) o[d] = rr[d] * A.Dinv[i];
+        } else {
+          dilu_bwd_row_g<NS>(A, rr, [&](int j, int d) -> T {
+            T rj[NS], zj[NS];
+#pragma unroll
+            for (int e = 0; e < NS; ++e) rj[e] = getr(j, e);
+            dilu_fwd_row<NS>(A, rj, getr, j, 0, zj);
+            return zj[d];
+          }, i, o);
+        }
         have = true;
+      } else {
+        have = precon_local<NS>(P, A, i, rr, o);
+        if (!have && lvl1 && __ldg(P.flev + i) == 1) {
+          dilu_fwd_row<NS>(A, rr, getr, i, __ldg(P.blev + i), o);
+          have = true;
+        }
       }
       if (have)
 #pragma unroll
@@ -533,7 +558,7 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
         for (int d = 0; d < NS; ++d) v[d] = (double)rr[d] * (double)o[d];
     });
     if (!C.sync()) return false;
-    if (dilu && !precon_tail<NS, NS>(C, A, (const T *)rn, zw, false, 2, [&](int i, double (&v)[NS]) {
+    if (dilu && !fuse && !precon_tail<NS, NS>(C, A, (const T *)rn, zw, false, 2, [&](int i, double (&v)[NS]) {
 #pragma unroll
           for (int d = 0; d < NS; ++d) v[d] = (double)rn[(size_t)i * NS + d] * (double)z[(size_t)i * NS + d];
         }))
@@ -1184,6 +1209,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
   for (int it = 0; it < iters; ++it) {
     done = it + 1;
     double Rit[4] = {1.0, 1.0, 1.0, 1.0};
+    bool finite = true;   // Krylov residual norms of this iteration all finite
     // ---- momentum: assemble, start Krylov, set up M, solve
     const MatT<T> &AUT = matU<T>(P);
     const KWorkT<T> &wU = workU<T>(P);
@@ -1197,6 +1223,8 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     int itsU[NS];
     double rnU[NS];
     if (!krylov<NS, T>(C, AUT, wU, P.bU, P.kU, P.kU.solver, itsU, rnU)) return;
+#pragma unroll
+    for (int d = 0; d < NS; ++d) finite = finite && isfinite(rnU[d]);
     // run! copy-back: U = x + x0
     tile_each(P, [&](int i) {
 #pragma unroll
@@ -1270,6 +1298,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       int itsP[1];
       double rnP[1];
       if (!krylov<1, T>(C, APT, wP, P.bP, P.kP, P.kP.solver, itsP, rnP)) return;
+      finite = finite && isfinite(rnP[0]);
       // run! copy-back then explicit_relaxation!(p, prev, alpha_p)
       tile_each(P, [&](int i) {
         const double pn = (double)wP.x[i] + P.p[i];
@@ -1303,10 +1332,20 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       if (!C.sync()) return;
       if (P.model == 1 && !turbulence<NS, T>(C)) return;
     }
+    // XCAL_FLAG_ABORT_ON_NAN (no reference counterpart): stop a diverged run.
+    // The residuals R_* themselves may be 0/0 = NaN on a healthy run (a zero
+    // right-hand side, e.g. uy at the first iteration), so the test uses the
+    // Krylov residual norms, which are finite whenever A, b and x0 are.
+    if (P.abort_nan) {
+      if (!finite) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) P.bar->nonfinite = 1;
+        break;
+      }
+    }
     if (!piso) {
       // convergence test (Solvers_1_SIMPLE.jl:200-215); every CTA holds the
       // same residual values, so all take the same branch
-      const double conv = 1e-7;
+      const double conv = P.conv;
       bool c = true;
 #pragma unroll
       for (int d = 0; d < NS; ++d) c = c && (Rit[d] <= conv);

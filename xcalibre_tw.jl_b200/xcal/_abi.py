@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "libxcal.so")
 
 # status codes
 XCAL_OK = 0
+XCAL_PENDING = 1
 ERRORS = {
     -1: "XCAL_ERR_ARG", -2: "XCAL_ERR_MESH", -3: "XCAL_ERR_OOM", -4: "XCAL_ERR_CUDA",
     -5: "XCAL_ERR_NAN", -6: "XCAL_ERR_TIMEOUT", -7: "XCAL_ERR_STATE", -8: "XCAL_ERR_IO",
@@ -29,7 +30,7 @@ MODEL_LAMINAR, MODEL_KOMEGA = 0, 1
 RENUMBER_NONE, RENUMBER_RCM, RENUMBER_COLOR = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 FIELD_UX, FIELD_UY, FIELD_UZ, FIELD_P, FIELD_K, FIELD_OMEGA, FIELD_NUT = range(7)
-FLAG_ABORT_ON_NAN, FLAG_PHASE_TIMERS = 1, 2
+FLAG_ABORT_ON_NAN, FLAG_PHASE_TIMERS, FLAG_CLUSTER = 1, 2, 4
 
 P_d = C.POINTER(C.c_double)
 P_i64 = C.POINTER(C.c_int64)
@@ -83,6 +84,23 @@ class Case(C.Structure):
     ]
 
 
+class ServeCfg(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("max_iterations", C.c_int32), ("renumber", C.c_int32),
+                ("pad", C.c_int32), ("tolerance", C.c_double)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("converged", C.c_int32),
+                ("ncells", C.c_int32), ("residual", C.c_double * 4), ("queue_ms", C.c_double),
+                ("setup_ms", C.c_double), ("run_ms", C.c_double), ("total_ms", C.c_double)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("queued", C.c_int64), ("running", C.c_int64), ("cell_iterations", C.c_double),
+                ("run_ms", C.c_double)]
+
+
 def dptr(a):
     return a.ctypes.data_as(P_d) if a is not None else None
 
@@ -129,6 +147,14 @@ SIGNATURES = {
     "xcal_residual": (C.c_int, [C.c_void_p, C.c_int64, P_i32, P_i32, P_d, P_d, P_d, P_d]),
     "xcal_residual_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p]),
+    "xcal_ctx_set_tolerance": (C.c_int, [C.c_void_p, C.c_double]),
+    "xcal_serve_create": (C.c_int, [C.c_int, C.POINTER(ServeCfg), C.POINTER(C.c_void_p)]),
+    "xcal_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(Case), P_d, P_d,
+                                    P_i64]),
+    "xcal_serve_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(ServeResult), P_d,
+                                  P_d]),
+    "xcal_serve_stats_get": (C.c_int, [C.c_void_p, C.POINTER(ServeStats)]),
+    "xcal_serve_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None

@@ -347,6 +347,10 @@ class Solver:
     def setup(self, case):
         _abi.check(self.lib.xcal_case_setup(self.ctx, C.byref(case)), self.ctx, "xcal_case_setup")
 
+    def set_tolerance(self, tol):
+        """SIMPLE stop tolerance (1e-7 as in the reference unless changed)."""
+        _abi.check(self.lib.xcal_ctx_set_tolerance(self.ctx, float(tol)), self.ctx, "xcal_ctx_set_tolerance")
+
     def set_field(self, which, values):
         v = np.ascontiguousarray(values, dtype=np.float64)
         _abi.check(self.lib.xcal_field_set(self.ctx, which, _abi.dptr(v), len(v)), self.ctx,
@@ -471,3 +475,70 @@ def piso(model, config, resume=True, pref=None, renumber=_abi.RENUMBER_COLOR, de
          precision=_abi.PREC_FP64):
     """piso!(model, config; resume, pref) -> (R_ux, R_uy, R_p); fields updated in place."""
     return _run(model, config, pref, True, renumber, device, precision)
+
+
+class Server:
+    """A stream of independent cases on one GPU (xcal_serve_*): `slots` worker
+    threads, each running its cases as one hardware cluster on its own stream,
+    every case until all residuals are <= tolerance or max_iterations."""
+
+    def __init__(self, device=0, slots=16, max_iterations=3000, tolerance=1e-6,
+                 renumber=_abi.RENUMBER_COLOR):
+        self.lib = _abi.load()
+        cfg = _abi.ServeCfg(slots=slots, max_iterations=max_iterations, renumber=renumber, pad=0,
+                            tolerance=tolerance)
+        h = C.c_void_p()
+        _abi.check(self.lib.xcal_serve_create(device, C.byref(cfg), C.byref(h)), None, "xcal_serve_create")
+        self.srv = h
+        self.ncells = {}
+
+    def submit(self, model, config, pref=None, precision=_abi.PREC_MIXED):
+        """Queue simple!(model, config; pref) with the model's current fields as
+        the initial condition; returns a ticket."""
+        mesh = model.mesh
+        case, keep = make_case(model, config, pref, precision)
+        n = mesh.ncells
+        U = np.ascontiguousarray(np.stack([model.U.x.values, model.U.y.values, model.U.z.values]).reshape(3 * n),
+                                 dtype=np.float64)
+        p = np.ascontiguousarray(model.p.values, dtype=np.float64)
+        t = C.c_int64()
+        _abi.check(self.lib.xcal_serve_submit(self.srv, C.byref(mesh.desc()), C.byref(case), _abi.dptr(U),
+                                              _abi.dptr(p), C.byref(t)), None, "xcal_serve_submit")
+        self.ncells[t.value] = n
+        return t.value
+
+    def poll(self, ticket, wait_ms=0):
+        """None while the case runs; then a dict with the result and fields."""
+        if ticket not in self.ncells:
+            raise _abi.XcalError(f"xcal_serve_poll: unknown or already collected ticket {ticket}")
+        n = self.ncells[ticket]
+        res = _abi.ServeResult()
+        U = np.zeros(3 * n)
+        p = np.zeros(n)
+        st = self.lib.xcal_serve_poll(self.srv, ticket, int(wait_ms), C.byref(res), _abi.dptr(U), _abi.dptr(p))
+        if st == _abi.XCAL_PENDING:
+            return None
+        _abi.check(st, None, "xcal_serve_poll")
+        del self.ncells[ticket]
+        out = {k: getattr(res, k) for k in ("status", "iterations", "converged", "ncells", "queue_ms",
+                                            "setup_ms", "run_ms", "total_ms")}
+        out["residual"] = list(res.residual)
+        out["U"] = U.reshape(3, n)
+        out["p"] = p
+        return out
+
+    def stats(self):
+        st = _abi.ServeStats()
+        _abi.check(self.lib.xcal_serve_stats_get(self.srv, C.byref(st)), None, "xcal_serve_stats_get")
+        return {k: getattr(st, k) for k, _ in _abi.ServeStats._fields_}
+
+    def close(self):
+        if getattr(self, "srv", None):
+            self.lib.xcal_serve_destroy(self.srv)
+            self.srv = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

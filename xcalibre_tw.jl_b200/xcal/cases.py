@@ -41,10 +41,10 @@ def solvers_for(model, p_solver=X.CgSolver, u_solver=X.BicgstabSolver, precon=X.
                        relax=relax_p, itmax=itmax))
 
 
-def cavity2d(n=40, iterations=1000, divergence=X.Upwind, gradient=X.Orthogonal, **kw):
-    path = _unv("cavity", meshgen.cavity_unv, n=n, L=0.1)
-    mesh = X.build_mesh(path)
-    model = X.RANS(X.Laminar, mesh=mesh, viscosity=X.ConstantScalar(1e-3))
+def cavity2d(n=40, iterations=1000, divergence=X.Upwind, gradient=X.Orthogonal, nu=1e-3, mesh=None, **kw):
+    if mesh is None:
+        mesh = X.build_mesh(_unv("cavity", meshgen.cavity_unv, n=n, L=0.1))
+    model = X.RANS(X.Laminar, mesh=mesh, viscosity=X.ConstantScalar(nu))
     X.assign(model, "U", X.Dirichlet("inlet", [0.0, 0.0, 0.0]), X.Dirichlet("outlet", [0.0, 0.0, 0.0]),
              X.Dirichlet("bottom", [0.0, 0.0, 0.0]), X.Dirichlet("top", [1.0, 0.0, 0.0]))
     X.assign(model, "p", *[X.Neumann(b, 0.0) for b in ("inlet", "outlet", "bottom", "top")])
@@ -57,10 +57,10 @@ def cavity2d(n=40, iterations=1000, divergence=X.Upwind, gradient=X.Orthogonal, 
     return mesh, model, config, 0.0
 
 
-def bfs(cells_per_h=27, iterations=2000, divergence=X.Upwind, gradient=X.Orthogonal, **kw):
-    path = _unv("bfs", meshgen.bfs_unv, cells_per_h=cells_per_h)
-    mesh = X.build_mesh(path)
-    model = X.RANS(X.Laminar, mesh=mesh, viscosity=X.ConstantScalar(1e-4))
+def bfs(cells_per_h=27, iterations=2000, divergence=X.Upwind, gradient=X.Orthogonal, nu=1e-4, mesh=None, **kw):
+    if mesh is None:
+        mesh = X.build_mesh(_unv("bfs", meshgen.bfs_unv, cells_per_h=cells_per_h))
+    model = X.RANS(X.Laminar, mesh=mesh, viscosity=X.ConstantScalar(nu))
     X.assign(model, "U", X.Dirichlet("inlet", [0.5, 0.0, 0.0]), X.Neumann("outlet", 0.0),
              X.Dirichlet("wall", [0.0, 0.0, 0.0]), X.Dirichlet("top", [0.0, 0.0, 0.0]))
     X.assign(model, "p", X.Neumann("inlet", 0.0), X.Dirichlet("outlet", 0.0), X.Neumann("wall", 0.0),
@@ -132,3 +132,36 @@ def flatplate(nx=600, ny=250, iterations=3000, wall_functions=False, **kw):
     X.initialise(model.turbulence.omega, win)
     X.initialise(model.turbulence.nut, kin / win)
     return mesh, model, config, None
+
+
+def serving_stream(n_cases=512, rate=20.0, seed=12345, nmin=40, nmax=400, p_bfs=0.5, re_max=1000.0):
+    """The serving workload: n_cases arrivals of a Poisson process (rate per
+    second), each a cavity or (probability p_bfs) a BFS case of about N x N
+    quads, N = round(exp(U(ln nmin, ln nmax))), Reynolds number U(50, re_max)
+    applied through the viscosity (lid 1 m/s over 0.1 m; inlet 0.5 m/s over
+    h = 10 mm).  The BFS gets N^2 cells split between its blocks by area
+    (5h x h inlet and 30h x 2h outlet: 65 c^2 cells for c cells per h).
+    Meshes are built once per (kind, size).  Returns a list of dicts with
+    arrival time t, kind, N, Re, mesh, model, config, pref."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, n_cases)
+    t = np.cumsum(gaps) - gaps[0]
+    meshes = {}
+    out = []
+    for k in range(n_cases):
+        is_bfs = rng.random() < p_bfs
+        N = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+        Re = float(rng.uniform(50.0, re_max))
+        if is_bfs:
+            c = max(2, int(round(N / np.sqrt(65.0))))
+            key = ("bfs", c)
+            if key not in meshes:
+                meshes[key] = X.build_mesh(_unv("bfs", meshgen.bfs_unv, cells_per_h=c))
+            mesh, model, config, pref = bfs(c, iterations=1, nu=0.5 * 0.01 / Re, mesh=meshes[key])
+        else:
+            key = ("cavity", N)
+            if key not in meshes:
+                meshes[key] = X.build_mesh(_unv("cavity", meshgen.cavity_unv, n=N, L=0.1))
+            mesh, model, config, pref = cavity2d(N, iterations=1, nu=1.0 * 0.1 / Re, mesh=meshes[key])
+        out.append(dict(t=float(t[k]), kind=key[0], N=N, Re=Re, mesh=mesh, model=model, config=config, pref=pref))
+    return out
