@@ -52,11 +52,12 @@ enum { XCAL_TIME_STEADY = 0, XCAL_TIME_EULER = 1 };
 enum { XCAL_DIV_LINEAR = 0, XCAL_DIV_UPWIND = 1 };
 enum { XCAL_LAP_LINEAR = 0 };
 enum { XCAL_GRAD_ORTHOGONAL = 0, XCAL_GRAD_MIDPOINT = 1 };
-/* Krylov solvers (Krylov.jl 0.9.5 CgSolver / BicgstabSolver) */
-enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
+/* Krylov solvers (Krylov.jl 0.9.5 CgSolver / BicgstabSolver / GmresSolver;
+ * GMRES without restart, itmax <= 1000) */
+enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1, XCAL_SOLVER_GMRES = 2 };
 /* preconditioners: src/Solve/Preconditioners/preconditioners_0_types.jl:7-12 */
 enum { XCAL_PRECON_DILU = 0, XCAL_PRECON_JACOBI = 1, XCAL_PRECON_NORMDIAG = 2,
-       XCAL_PRECON_NONE = 3 };
+       XCAL_PRECON_NONE = 3, XCAL_PRECON_ILU0 = 4 /* ILUZero.jl 0.2.0 ilu0 */ };
 /* turbulence model: src/RANSModels/RANSModels_0_types.jl:10, RANSModels_kOmega.jl:127 */
 enum { XCAL_MODEL_LAMINAR = 0, XCAL_MODEL_KOMEGA = 1 };
 /* cell renumbering applied once at mesh upload */

@@ -48,6 +48,7 @@ def lib():
         L.orc_linear_solve.argtypes = [C.c_int32, C.c_int32, C.c_int64, P_i32, P_i32, P_d, P_d,
                                        P_d, C.c_int32, C.c_double, C.c_double, P_i32, P_d]
         L.orc_dilu_apply.argtypes = [C.c_int64, P_i32, P_i32, P_d, P_d, P_d, P_d]
+        L.orc_precon_apply.argtypes = [C.c_int32, C.c_int64, P_i32, P_i32, P_d, P_d, P_d]
         L.orc_residual.argtypes = [C.c_int64, P_i32, P_i32, P_d, P_d, P_d]
         L.orc_residual.restype = C.c_double
         L.orc_canon_dot.argtypes = [C.c_int64, P_d, P_d]
@@ -165,6 +166,19 @@ def linear_solve(solver, precon, row_ptr, col, val, b, x0, itmax=100, atol=1.490
                            _abi.dptr(bb), _abi.dptr(x), itmax, atol, rtol, _abi.i32ptr(it),
                            _abi.dptr(rn))
     return x, int(it[0]), float(rn[0])
+
+
+def precon_apply(precon, row_ptr, col, val, b):
+    """y = M^{-1} b for a CSR matrix (update_preconditioner! then ldiv!)."""
+    n = len(b)
+    y = np.zeros(n)
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    vv = np.ascontiguousarray(val, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    lib().orc_precon_apply(precon, n, _abi.i32ptr(rp), _abi.i32ptr(cl), _abi.dptr(vv), _abi.dptr(bb),
+                           _abi.dptr(y))
+    return y
 
 
 def dilu_apply(row_ptr, col, val, b):

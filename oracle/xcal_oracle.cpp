@@ -21,6 +21,14 @@
 //     which Krylov.jl's CG takes sqrt of a negative <r,z> and throws.  CG is run
 //     on the negated system (-A)x = -b, which is mathematically the same solve;
 //     negation is exact, so this equals flipping the sign of <r,z> and <p,Ap>.
+//   * GMRES (Krylov.jl 0.9.5 gmres!, restart = false, left preconditioner M,
+//     modified Gram-Schmidt, Givens QR via sym_givens (SymOrtho), back
+//     substitution, x = V y) restated from the same published algorithm.
+//   * ILU0 (ILUZero.jl 0.2.0, not vendored): ILU(0) in the IKJ form with L
+//     entries scaled by the reciprocal of the pivot; ldiv! as unit-lower
+//     forward substitution (ascending columns) and upper backward substitution
+//     subtracting in descending column order before dividing by the diagonal
+//     (the order of a column-oriented CSC sweep).
 //   * DILU's O(n^2) upper_row_indices is built in O(nnz) with identical output.
 //   * The "3D extension" (dim == 3): the reference is 2D-only; the same formulas
 //     carried to the z component (uz equation, 3-component interpolation, H and
@@ -534,10 +542,36 @@ struct Precon {
   std::vector<double> D;            // DILU: inverse pivots after update; Jacobi/NormDiag: scale
   std::vector<i64> Di;
   std::vector<std::vector<i64>> Ri, J;
+  // ILU(0): CSR view of the pattern (ascending columns), its CSC positions,
+  // diagonal positions and the factor values (L strictly lower, U upper)
+  std::vector<i64> rp, cl, cpos, dp;
+  std::vector<double> F;
+  i64 find(i64 r, i64 c) const {
+    for (i64 e = rp[r]; e < rp[r + 1]; ++e) {
+      if (cl[e] == c) return e;
+      if (cl[e] > c) break;
+    }
+    return -1;
+  }
   void setup(int t, const CSC *Am) {
     type = t; A = Am;
     i64 n = A->n;
     D.assign(n, 0.0);
+    if (type == XCAL_PRECON_ILU0) {
+      rp.assign(n + 1, 0);
+      for (i64 j = 0; j < n; ++j) for (i64 p = A->colptr[j]; p < A->colptr[j + 1]; ++p) rp[A->rowval[p] + 1]++;
+      for (i64 i = 0; i < n; ++i) rp[i + 1] += rp[i];
+      cl.assign(rp[n], 0); cpos.assign(rp[n], 0); dp.assign(n, -1);
+      std::vector<i64> fill(rp.begin(), rp.end() - 1);
+      for (i64 j = 0; j < n; ++j)
+        for (i64 p = A->colptr[j]; p < A->colptr[j + 1]; ++p) {
+          i64 r = A->rowval[p], e = fill[r]++;
+          cl[e] = j; cpos[e] = p;
+          if (r == j) dp[r] = e;
+        }
+      F.assign(rp[n], 0.0);
+      return;
+    }
     if (type != XCAL_PRECON_DILU) return;
     Di.assign(n, 0);   // diagonal_indices! :159-174
     i64 idx = 0;
@@ -568,6 +602,19 @@ struct Precon {
         }
         D[i] = 1 / D[i];
       }
+    } else if (type == XCAL_PRECON_ILU0) {   // ilu0!(P.storage, P.A), preconditioners_2_functions.jl:59-65
+      for (size_t e = 0; e < F.size(); ++e) F[e] = a.nzval[cpos[e]];
+      for (i64 i = 0; i < n; ++i)
+        for (i64 e = rp[i]; e < rp[i + 1]; ++e) {
+          i64 k = cl[e];
+          if (k >= i) break;
+          const double l = F[e] * (1.0 / F[dp[k]]);
+          F[e] = l;
+          for (i64 m = e + 1; m < rp[i + 1]; ++m) {
+            i64 pos = find(k, cl[m]);
+            if (pos >= 0) F[m] = F[m] - l * F[pos];
+          }
+        }
     } else if (type == XCAL_PRECON_JACOBI) {   // preconditioners_2_functions.jl:43-57
       for (i64 i = 0; i < n; ++i) D[i] = 1 / std::fabs(a.nzval[a.pos(i, i)]);
     } else if (type == XCAL_PRECON_NORMDIAG) {   // :28-41
@@ -593,6 +640,18 @@ struct Precon {
       for (i64 i = n - 2; i >= 0; --i)
         for (size_t pi = 0; pi < Ri[i].size(); ++pi)
           x[i] -= a.nzval[Ri[i][pi]] * x[J[i][pi]] * D[i];
+    } else if (type == XCAL_PRECON_ILU0) {   // ldiv!(y, LU, v)
+      std::vector<double> y(n);
+      for (i64 i = 0; i < n; ++i) {
+        double v = b[i];
+        for (i64 e = rp[i]; e < rp[i + 1] && cl[e] < i; ++e) v = v - F[e] * y[cl[e]];
+        y[i] = v;
+      }
+      for (i64 i = n - 1; i >= 0; --i) {
+        double v = y[i];
+        for (i64 e = rp[i + 1] - 1; e >= rp[i] && cl[e] > i; --e) v = v - F[e] * x[cl[e]];
+        x[i] = v / F[dp[i]];
+      }
     } else if (type == XCAL_PRECON_NONE) {
       for (i64 i = 0; i < n; ++i) x[i] = b[i];
     } else {
@@ -705,9 +764,104 @@ static int krylov_bicgstab(const CSC &A, const std::vector<double> &b, std::vect
   return iter;
 }
 
+// SymOrtho plane rotation (Choi, Paige & Saunders), Krylov.jl sym_givens
+static void sym_givens(double a, double b, double &c, double &s, double &rho) {
+  auto sgn = [](double v) { return v > 0.0 ? 1.0 : (v < 0.0 ? -1.0 : v); };
+  if (b == 0.0) {
+    c = (a == 0.0) ? 1.0 : sgn(a);
+    s = 0.0;
+    rho = std::fabs(a);
+  } else if (a == 0.0) {
+    c = 0.0;
+    s = sgn(b);
+    rho = std::fabs(b);
+  } else if (std::fabs(b) > std::fabs(a)) {
+    double t = a / b;
+    s = sgn(b) / std::sqrt(1.0 + t * t);
+    c = s * t;
+    rho = b / s;
+  } else {
+    double t = b / a;
+    c = sgn(a) / std::sqrt(1.0 + t * t);
+    s = c * t;
+    rho = a / c;
+  }
+}
+
+// gmres! (restart = false, reorthogonalization = false, N = I)
+static int krylov_gmres(const CSC &A, const std::vector<double> &b, std::vector<double> &values,
+                        const Precon &M, int itmax, double atol, double rtol, double *rnorm_out) {
+  i64 n = A.n;
+  std::vector<double> dx = values, x(n, 0.0), w(n), r0(n), q(n);
+  spmv(A, dx, w);
+  for (i64 i = 0; i < n; ++i) w[i] = b[i] - w[i];        // w = b - A*Δx
+  M.apply(w, r0);                                          // r0 = M w
+  double beta = cnrm2(r0), rNorm = beta;
+  const double btol = 1.8189894035458565e-12;             // eps^(3/4) = 2^-39
+  int iter = 0;
+  if (beta == 0.0) {
+    for (i64 i = 0; i < n; ++i) values[i] = x[i] + dx[i];
+    if (rnorm_out) *rnorm_out = rNorm;
+    return 0;
+  }
+  double epsl = atol + rtol * rNorm;
+  bool solved = rNorm <= epsl, tired = iter >= itmax;
+  if (!(solved || tired)) {
+    std::vector<std::vector<double>> V(1, std::vector<double>(n));
+    std::vector<double> R, c, s, z(1, beta);
+    for (i64 i = 0; i < n; ++i) V[0][i] = r0[i] / rNorm;
+    int k = 0;
+    bool inner_tired = false, breakdown = false;
+    size_t nr = 0;
+    while (!(solved || inner_tired || breakdown)) {
+      ++k;
+      R.resize(nr + k, 0.0); c.resize(k, 0.0); s.resize(k, 0.0);
+      spmv(A, V[k - 1], w);
+      M.apply(w, q);
+      for (int i = 0; i < k; ++i) {                        // modified Gram-Schmidt
+        R[nr + i] = cdot(V[i], q);
+        for (i64 j = 0; j < n; ++j) q[j] = q[j] + (-R[nr + i]) * V[i][j];
+      }
+      double Hbis = cnrm2(q);
+      for (int i = 0; i < k - 1; ++i) {
+        double tmp = c[i] * R[nr + i] + s[i] * R[nr + i + 1];
+        R[nr + i + 1] = s[i] * R[nr + i] - c[i] * R[nr + i + 1];
+        R[nr + i] = tmp;
+      }
+      sym_givens(R[nr + k - 1], Hbis, c[k - 1], s[k - 1], R[nr + k - 1]);
+      double zeta = s[k - 1] * z[k - 1];
+      z[k - 1] = c[k - 1] * z[k - 1];
+      rNorm = std::fabs(zeta);
+      nr += k;
+      iter++;
+      bool mach = (rNorm + 1.0 <= 1.0);
+      solved = (rNorm <= epsl) || mach;
+      breakdown = Hbis <= btol;
+      inner_tired = k >= itmax;
+      if (!(solved || inner_tired || breakdown)) {
+        V.emplace_back(n);
+        for (i64 i = 0; i < n; ++i) V[k][i] = q[i] / Hbis;
+        z.push_back(zeta);
+      }
+    }
+    std::vector<double> y(z.begin(), z.begin() + k);       // back substitution R y = z
+    for (int i = k - 1; i >= 0; --i) {
+      for (int j = k - 1; j >= i + 1; --j) y[i] = y[i] - R[(size_t)j * (j + 1) / 2 + i] * y[j];
+      double rii = R[(size_t)i * (i + 1) / 2 + i];
+      y[i] = (std::fabs(rii) <= btol) ? 0.0 : y[i] / rii;
+    }
+    for (int i = 0; i < k; ++i)
+      for (i64 j = 0; j < n; ++j) x[j] = x[j] + y[i] * V[i][j];
+  }
+  for (i64 i = 0; i < n; ++i) values[i] = x[i] + dx[i];
+  if (rnorm_out) *rnorm_out = rNorm;
+  return iter;
+}
+
 static int krylov_solve(int solver, const CSC &A, const std::vector<double> &b, std::vector<double> &x,
                         const Precon &M, int itmax, double atol, double rtol, double *rn) {
   if (solver == XCAL_SOLVER_CG) return krylov_cg(A, b, x, M, itmax, atol, rtol, rn);
+  if (solver == XCAL_SOLVER_GMRES) return krylov_gmres(A, b, x, M, itmax, atol, rtol, rn);
   return krylov_bicgstab(A, b, x, M, itmax, atol, rtol, rn);
 }
 
@@ -1458,6 +1612,26 @@ int orc_linear_solve(int32_t solver, int32_t precon, int64_t n, const int32_t *r
   std::copy(xx.begin(), xx.end(), x);
   if (niter) *niter = it;
   if (rnorm) *rnorm = rn;
+  return XCAL_OK;
+}
+
+// Any preconditioner applied once (update_preconditioner! + ldiv!), CSR input.
+int orc_precon_apply(int32_t precon, int64_t n, const int32_t *rp, const int32_t *col, const double *val,
+                     const double *b, double *y) {
+  CSC A; A.n = n; A.colptr.assign(n + 1, 0);
+  for (i64 i = 0; i < n; ++i) for (int32_t q = rp[i]; q < rp[i + 1]; ++q) A.colptr[col[q] + 1]++;
+  for (i64 j = 0; j < n; ++j) A.colptr[j + 1] += A.colptr[j];
+  A.rowval.assign(A.colptr[n], 0); A.nzval.assign(A.colptr[n], 0.0);
+  std::vector<i64> fill(A.colptr.begin(), A.colptr.end() - 1);
+  for (i64 i = 0; i < n; ++i)
+    for (int32_t q = rp[i]; q < rp[i + 1]; ++q) {
+      i64 j = col[q], pos = fill[j]++;
+      A.rowval[pos] = i; A.nzval[pos] = val[q];
+    }
+  Precon M; M.setup(precon, &A); M.update();
+  std::vector<double> bb(b, b + n), yy(n, 0.0);
+  M.apply(bb, yy);
+  std::copy(yy.begin(), yy.end(), y);
   return XCAL_OK;
 }
 

@@ -111,13 +111,18 @@ def _snapshot_matrix(n=24, iters=5):
     return colptr.astype(np.int32), rowval.astype(np.int32), out
 
 
-@pytest.mark.parametrize("solver", [_abi.SOLVER_CG, _abi.SOLVER_BICGSTAB], ids=["cg", "bicgstab"])
-@pytest.mark.parametrize("precon", [_abi.PRECON_DILU, _abi.PRECON_JACOBI, _abi.PRECON_NONE],
-                         ids=["dilu", "jacobi", "none"])
-def test_linear_solve_parity(solver, precon):
-    """run! on a standalone CSR system (the cavity's pressure matrix)."""
+@pytest.mark.parametrize("solver", [_abi.SOLVER_CG, _abi.SOLVER_BICGSTAB, _abi.SOLVER_GMRES],
+                         ids=["cg", "bicgstab", "gmres"])
+@pytest.mark.parametrize("precon", [_abi.PRECON_DILU, _abi.PRECON_ILU0, _abi.PRECON_JACOBI, _abi.PRECON_NONE],
+                         ids=["dilu", "ilu0", "jacobi", "none"])
+@pytest.mark.parametrize("matrix", ["Ap", "AU"])
+def test_linear_solve_parity(solver, precon, matrix):
+    """run! on a standalone CSR system: the cavity's pressure matrix (symmetric)
+    and its momentum matrix (upwind convection, nonsymmetric)."""
+    if solver == _abi.SOLVER_CG and matrix == "AU":
+        pytest.skip("CG needs a symmetric system")
     rp, col, out = _snapshot_matrix()
-    A = out["Ap"]
+    A = out[matrix]
     n = len(rp) - 1
     rng = np.random.default_rng(7)
     b = rng.standard_normal(n)
@@ -139,6 +144,20 @@ def test_linear_solve_parity(solver, precon):
     assert int(it[0]) == ito
     assert np.linalg.norm(x - xo) <= TOL * np.linalg.norm(xo)
     assert rn[0] == rno or abs(rn[0] - rno) <= TOL * abs(rno)
+
+
+@pytest.mark.parametrize("u_solver,p_solver,precon", [
+    (X.GmresSolver, X.CgSolver, X.ILU0),
+    (X.GmresSolver, X.GmresSolver, X.DILU),
+    (X.BicgstabSolver, X.CgSolver, X.ILU0),
+], ids=["gmres-ilu0", "gmres-gmres-dilu", "bicgstab-cg-ilu0"])
+def test_gmres_ilu0_simple_parity(u_solver, p_solver, precon):
+    """simple! with GmresSolver and ILU0() as in the reference's case scripts
+    (CASE_UNV_BFS.jl, CASE_cylinder_U.jl): 30 iterations on a jittered BFS."""
+    mesh, model, config, pref = cases.bfs(5, iterations=30, u_solver=u_solver, p_solver=p_solver, precon=precon)
+    dev = run_device(mesh, model, config, pref, 30, _abi.RENUMBER_COLOR)
+    orc = run_oracle(dev["dev_mesh"], model, config, pref, 30, dev["perm"])
+    assert_parity(dev, orc)
 
 
 def test_field_roundtrip_and_permutation():

@@ -143,3 +143,103 @@ def test_golden_regression():
     for k in ("R_ux", "R_p"):
         assert np.array_equal(out[k], g[k])
     assert np.array_equal(out["U"], g["U"]) and np.array_equal(out["p"], g["p"])
+
+
+def _laplace_csr(nx, ny, shift=0.0, skew=0.0):
+    """5-point operator on an nx x ny grid (rows in natural order), optionally
+    with a diagonal shift and an antisymmetric convection-like skew."""
+    n = nx * ny
+    rows = []
+    for j in range(ny):
+        for i in range(nx):
+            r = j * nx + i
+            ent = {r: 4.0 + shift}
+            for di, dj, sgn in ((-1, 0, 1), (1, 0, -1), (0, -1, 1), (0, 1, -1)):
+                ii, jj = i + di, j + dj
+                if 0 <= ii < nx and 0 <= jj < ny:
+                    ent[jj * nx + ii] = -1.0 + sgn * skew
+            rows.append(sorted(ent.items()))
+    rp = np.zeros(n + 1, dtype=np.int32)
+    col, val = [], []
+    for r, ent in enumerate(rows):
+        for c, v in ent:
+            col.append(c)
+            val.append(v)
+        rp[r + 1] = len(col)
+    return rp, np.array(col, dtype=np.int32), np.array(val)
+
+
+def test_ilu0_matches_independent_ikj():
+    """The oracle's ILU(0) equals a direct dense IKJ ILU(0) restricted to the
+    pattern (Saad, Iterative Methods, Alg. 10.4) with the same operation order."""
+    rp, col, val = _laplace_csr(5, 4, shift=0.3, skew=0.2)
+    n = len(rp) - 1
+    pat = {(r, int(col[q])) for r in range(n) for q in range(rp[r], rp[r + 1])}
+    F = np.zeros((n, n))
+    for r in range(n):
+        for q in range(rp[r], rp[r + 1]):
+            F[r, col[q]] = val[q]
+    for i in range(n):
+        for k in range(i):
+            if (i, k) not in pat:
+                continue
+            F[i, k] = F[i, k] * (1.0 / F[k, k])
+            for j in range(k + 1, n):
+                if (i, j) in pat and (k, j) in pat:
+                    F[i, j] = F[i, j] - F[i, k] * F[k, j]
+    b = np.random.default_rng(3).standard_normal(n)
+    y = np.zeros(n)
+    for i in range(n):
+        v = b[i]
+        for k in range(i):
+            if (i, k) in pat:
+                v = v - F[i, k] * y[k]
+        y[i] = v
+    x = np.zeros(n)
+    for i in range(n - 1, -1, -1):
+        v = y[i]
+        for j in range(n - 1, i, -1):
+            if (i, j) in pat:
+                v = v - F[i, j] * x[j]
+        x[i] = v / F[i, i]
+    assert np.array_equal(O.precon_apply(_abi.PRECON_ILU0, rp, col, val, b), x)
+
+
+def test_ilu0_exact_on_tridiagonal_and_gmres_one_step():
+    """ILU(0) of a tridiagonal matrix has no dropped fill, so it is the exact LU:
+    M^{-1} A = I and preconditioned GMRES converges in one iteration."""
+    rp, col, val = _laplace_csr(12, 1, shift=0.5, skew=0.3)
+    n = len(rp) - 1
+    A = np.zeros((n, n))
+    for r in range(n):
+        A[r, col[rp[r]:rp[r + 1]]] = val[rp[r]:rp[r + 1]]
+    b = np.arange(1.0, n + 1)
+    y = O.precon_apply(_abi.PRECON_ILU0, rp, col, val, b)
+    assert np.allclose(A @ y, b, rtol=0, atol=1e-12)
+    x, it, rn = O.linear_solve(_abi.SOLVER_GMRES, _abi.PRECON_ILU0, rp, col, val, b, np.zeros(n),
+                               itmax=20, rtol=1e-12)
+    assert it == 1 and np.allclose(A @ x, b, rtol=0, atol=1e-10)
+
+
+@pytest.mark.parametrize("precon", [_abi.PRECON_NONE, _abi.PRECON_JACOBI, _abi.PRECON_DILU, _abi.PRECON_ILU0])
+def test_gmres_solves_nonsymmetric_system(precon):
+    """Full GMRES (no restart) on a nonsymmetric 2D convection-diffusion
+    operator: converges within n iterations to the direct solution, with
+    warm start, and reports iterations <= itmax."""
+    rp, col, val = _laplace_csr(7, 6, shift=0.1, skew=0.35)
+    n = len(rp) - 1
+    A = np.zeros((n, n))
+    for r in range(n):
+        A[r, col[rp[r]:rp[r + 1]]] = val[rp[r]:rp[r + 1]]
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(n)
+    x0 = 0.1 * rng.standard_normal(n)
+    x, it, rn = O.linear_solve(_abi.SOLVER_GMRES, precon, rp, col, val, b, x0, itmax=n, atol=1e-13,
+                               rtol=1e-13)
+    xd = np.linalg.solve(A, b)
+    assert 1 <= it <= n
+    assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+    # itmax caps the basis: 3 iterations, residual reported > tolerance
+    x3, it3, rn3 = O.linear_solve(_abi.SOLVER_GMRES, precon, rp, col, val, b, x0, itmax=3, atol=1e-13,
+                                  rtol=1e-13)
+    assert it3 == 3 and rn3 > 1e-13

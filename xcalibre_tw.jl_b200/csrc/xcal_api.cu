@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -454,14 +455,34 @@ static int build_bc(xcal_ctx c, DevBuf &B, const xcal_bc *bcs, int nbc, FieldBC 
   return XCAL_OK;
 }
 
+constexpr int GMRES_MAX = 1000;   // GMRES basis limit (no restart: itmax vectors)
+
 static int check_solver(xcal_ctx c, const xcal_solver_cfg &s, const char *what) {
-  if (s.solver != XCAL_SOLVER_CG && s.solver != XCAL_SOLVER_BICGSTAB)
+  if (s.solver != XCAL_SOLVER_CG && s.solver != XCAL_SOLVER_BICGSTAB && s.solver != XCAL_SOLVER_GMRES)
     return fail(c, XCAL_ERR_UNSUPPORTED, std::string("solver not available for ") + what);
-  if (s.preconditioner < XCAL_PRECON_DILU || s.preconditioner > XCAL_PRECON_NONE)
+  if (s.preconditioner < XCAL_PRECON_DILU || s.preconditioner > XCAL_PRECON_ILU0)
     return fail(c, XCAL_ERR_UNSUPPORTED, std::string("preconditioner not available for ") + what);
   if (s.itmax < 0) return fail(c, XCAL_ERR_ARG, std::string("itmax < 0 for ") + what);
+  if (s.solver == XCAL_SOLVER_GMRES && s.itmax > GMRES_MAX)
+    return fail(c, XCAL_ERR_UNSUPPORTED, std::string("GMRES itmax above 1000 for ") + what);
   return XCAL_OK;
 }
+
+// GMRES work space of one Krylov work set (basis of gmax+1 vectors of m values,
+// per-CTA Givens scratch, packed R) and ILU(0) factor storage.
+}  // extern "C"
+template <class T, class AllocT>
+static void gmres_alloc(KWorkT<T> &w, int gmax, size_t m, int ns, int nblocks, AllocT allocT,
+                        double *&gws, double *&gR, const std::function<double *(size_t)> &allocD) {
+  w.gmax = gmax;
+  if (gmax <= 0) return;
+  w.V = allocT((size_t)(gmax + 1) * m);
+  if (!gws) gws = allocD((size_t)std::max(nblocks, 1) * ns * 4 * (gmax + 1));
+  if (!gR) gR = allocD((size_t)ns * gmax * (gmax + 1) / 2);
+  w.gws = gws;
+  w.gR = gR;
+}
+extern "C" {
 
 int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   if (!c || !cfg) return XCAL_ERR_ARG;
@@ -524,6 +545,20 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
     for (int b = 0; b < 2; ++b) { w->r[b] = A(m); w->p[b] = A(m); w->v[b] = A(m); }
   }
   h.part = A((size_t)MAXK * h.ntiles);
+  // ILU(0) factors and GMRES work space where a solver asks for them (k and
+  // omega reuse the pressure matrix and work set)
+  auto is_ilu = [](const xcal_solver_cfg &sc) { return sc.preconditioner == XCAL_PRECON_ILU0; };
+  auto gm = [](const xcal_solver_cfg &sc) { return sc.solver == XCAL_SOLVER_GMRES ? sc.itmax : 0; };
+  const bool iluU = is_ilu(cfg->solver_U);
+  const bool iluP = is_ilu(cfg->solver_p) || (turb && (is_ilu(cfg->solver_k) || is_ilu(cfg->solver_omega)));
+  const int gmU = gm(cfg->solver_U);
+  const int gmP = std::max(gm(cfg->solver_p), turb ? std::max(gm(cfg->solver_k), gm(cfg->solver_omega)) : 0);
+  h.AU.fval = iluU ? A(nnz) : nullptr;
+  h.AP.fval = iluP ? A(nnz) : nullptr;
+  double *gwsU = nullptr, *gRU = nullptr, *gwsP = nullptr, *gRP = nullptr;
+  std::function<double *(size_t)> allocD = [&](size_t cnt) { return A(cnt); };
+  gmres_alloc(h.wU, gmU, (size_t)n * NS, NS, c->nblocks, A, gwsU, gRU, allocD);
+  gmres_alloc(h.wP, gmP, (size_t)n, 1, c->nblocks, A, gwsP, gRP, allocD);
   h.prec = cfg->precision;
   if (h.prec == XCAL_PREC_MIXED) {
     auto F = [&](size_t cnt) { float *p = B.alloc<float>(cnt); if (!p) ok = false; return p; };
@@ -533,10 +568,14 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
       M32.col = M64.col; M32.tpos = M64.tpos; M32.dpos = M64.dpos; M32.W = M64.W; M32.np = M64.np;
       M32.precon = M64.precon;
       M32.val = F(nnz); M32.Dpiv = F(n); M32.Dinv = F(n);
+      M32.fval = M64.fval ? F(nnz) : nullptr;
       KWorkT<float> *w = (k == 0) ? &h.wU32 : &h.wP32;
       size_t m = (k == 0) ? (size_t)n * NS : (size_t)n;
       w->x = F(m); w->s = F(m); w->t = F(m); w->q = F(m);
       for (int b = 0; b < 2; ++b) { w->r[b] = F(m); w->p[b] = F(m); w->v[b] = F(m); }
+      const KWork &w64 = (k == 0) ? h.wU : h.wP;
+      double *g1 = w64.gws, *g2 = w64.gR;
+      gmres_alloc(*w, w64.gmax, m, (k == 0) ? NS : 1, c->nblocks, F, g1, g2, allocD);
     }
   }
   if (turb) {
@@ -729,9 +768,11 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
                       const int32_t *col, const double *val, const double *b, double *x, int32_t itmax,
                       double atol, double rtol, int32_t *niter, double *final_rnorm) {
   if (!c || !row_ptr || !col || !val || !b || !x || n64 <= 0 || n64 > (1 << 30)) return XCAL_ERR_ARG;
-  if (solver != XCAL_SOLVER_CG && solver != XCAL_SOLVER_BICGSTAB) return fail(c, XCAL_ERR_UNSUPPORTED, "solver");
-  if (precon < XCAL_PRECON_DILU || precon > XCAL_PRECON_NONE) return fail(c, XCAL_ERR_UNSUPPORTED, "preconditioner");
-  if (itmax < 0) return fail(c, XCAL_ERR_ARG, "itmax < 0");
+  {
+    xcal_solver_cfg sc{};
+    sc.solver = solver; sc.preconditioner = precon; sc.itmax = itmax;
+    TRY(check_solver(c, sc, "xcal_linear_solve"));
+  }
   CUDA_TRY(c, cudaSetDevice(c->device));
   int n = (int)n64;
   if (row_ptr[0] != 0) return fail(c, XCAL_ERR_ARG, "row_ptr[0] must be 0");
@@ -796,6 +837,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   bool ok = true;
   auto A = [&](size_t cnt) { double *p = B.alloc<double>(cnt); if (!p) ok = false; return p; };
   h.AU.Dpiv = A(n); h.AU.Dinv = A(n);
+  h.AU.fval = (precon == XCAL_PRECON_ILU0) ? A(ev.size()) : nullptr;
   KWork &w = h.wU;
   w.x = A(n); w.s = A(n); w.t = A(n); w.q = A(n);
   for (int k = 0; k < 2; ++k) { w.r[k] = A(n); w.p[k] = A(n); w.v[k] = A(n); }
@@ -815,6 +857,12 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
     c->ns = saved_ns; c->mode = saved_mode; c->nblocks = saved_nb;
   }
   h.mode = mode;
+  if (solver == XCAL_SOLVER_GMRES) {
+    double *g1 = nullptr, *g2 = nullptr;
+    std::function<double *(size_t)> allocD = [&](size_t cnt) { return A(cnt); };
+    gmres_alloc(h.wU, itmax, (size_t)n, 1, nb, A, g1, g2, allocD);
+    if (!ok) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+  }
   CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
   CUDA_TRY(c, launch_program(1, 0, mode, nb, &h, PROG_SOLVE, 1, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));

@@ -60,6 +60,7 @@ struct MatT {
   const int *dpos;      // [np] position of the diagonal entry
   T *val;               // [W*np]
   T *Dpiv, *Dinv;       // DILU pivots and their inverses (or the diagonal scaling)
+  T *fval;              // [W*np] ILU(0) factors: strict lower part L (unit diagonal), upper part U
   int precon, W, np;
 };
 using Mat = MatT<double>;
@@ -75,6 +76,12 @@ struct KCfg {
 template <typename T>
 struct KWorkT {
   T *x, *r[2], *p[2], *v[2], *s, *t, *q;
+  // GMRES: Krylov basis V (vector k at V + k*n*NS, gmax+1 vectors), per-CTA
+  // Givens scratch (NS x 4 x (gmax+1) doubles per CTA: c, s, z, column) and
+  // the packed triangular factor R (NS x gmax*(gmax+1)/2, written by CTA 0).
+  T *V;
+  double *gws, *gR;
+  int gmax;
 };
 using KWork = KWorkT<double>;
 
@@ -90,9 +97,9 @@ struct KParams {
   const int *cb_ptr, *cb_face;
   const int *flev, *blev;                 // [np]
   int nfl, nbl;
-  int cg_fuse;
-  int abort_nan;   // stop at the first non-finite residual
-  double conv;   // SIMPLE stop: every residual <= conv (1e-7 in the reference)   // CG: M^{-1} of a two-level DILU inside the x/r phase (2 barriers per iteration)
+  int cg_fuse;     // CG: M^{-1} of a two-level DILU inside the x/r phase (2 barriers per iteration)
+  int abort_nan;   // stop at the first non-finite Krylov residual norm
+  double conv;     // SIMPLE stop: every residual <= conv (1e-7 in the reference)
   Mat AU, AP;
   FieldBC bcU, bcP;
   // configuration
@@ -397,6 +404,93 @@ __device__ __forceinline__ void dilu_bwd_row(const MatT<T> &A, const T *out, int
 #pragma unroll
   for (int d = 0; d < NS; ++d) oi[d] = out[(size_t)i * NS + d];
   dilu_bwd_row_g<NS>(A, oi, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, o);
+}
+
+// ILU(0) (ILUZero.jl 0.2.0, preconditioners_0_types.jl:44-52 and
+// preconditioners_2_functions.jl:59-65; the package is not vendored, so this
+// restates the published algorithm).  Factor row i in level order (rows k < i
+// are final): F_i = A_i, then for each lower entry k in ascending column order
+// l_ik = F_ik * (1/F_kk) and F_ij -= l_ik * F_kj for every later entry j of
+// row i present in row k.  Apply: y = L^{-1} v with unit diagonal (ascending
+// k), then x_i = (y_i - sum_{j>i} F_ij x_j) / F_ii with the sum taken in
+// descending j (the column-oriented backward sweep).
+template <typename T>
+__device__ __forceinline__ T ell_find(const MatT<T> &A, const T *vals, int row, int colj) {
+  for (int k = 0; k < A.W; ++k) {
+    const int c = __ldg(A.col + (size_t)k * A.np + row);
+    if (c == colj) return vals[(size_t)k * A.np + row];
+    if (c < 0 || c > colj) break;
+  }
+  return T(0);
+}
+template <typename T>
+__device__ __forceinline__ bool ell_has(const MatT<T> &A, int row, int colj) {
+  for (int k = 0; k < A.W; ++k) {
+    const int c = __ldg(A.col + (size_t)k * A.np + row);
+    if (c == colj) return true;
+    if (c < 0 || c > colj) break;
+  }
+  return false;
+}
+
+template <typename T>
+__device__ __forceinline__ void ilu_setup_row(const MatT<T> &A, int i) {
+  for (int k = 0; k < A.W; ++k) {
+    const size_t e = (size_t)k * A.np + i;
+    A.fval[e] = A.val[e];
+  }
+  for (int k = 0; k < A.W; ++k) {
+    const size_t e = (size_t)k * A.np + i;
+    const int kk = __ldg(A.col + e);
+    if (kk < 0 || kk >= i) break;
+    const T ukk = A.fval[__ldg(A.dpos + kk)];
+    const T l = A.fval[e] * (T(1) / ukk);
+    A.fval[e] = l;
+    for (int m = k + 1; m < A.W; ++m) {
+      const size_t em = (size_t)m * A.np + i;
+      const int j = __ldg(A.col + em);
+      if (j < 0) break;
+      if (ell_has(A, kk, j)) A.fval[em] = A.fval[em] - l * ell_find(A, (const T *)A.fval, kk, j);
+    }
+  }
+}
+
+template <int NS, typename T, class GetOut>
+__device__ __forceinline__ void ilu_fwd_row(const MatT<T> &A, const T (&in)[NS], GetOut geto, int i, int blev_i,
+                                            T (&o)[NS]) {
+#pragma unroll
+  for (int d = 0; d < NS; ++d) o[d] = in[d];
+  for (int k = 0; k < A.W; ++k) {
+    const size_t e = (size_t)k * A.np + i;
+    const int j = __ldg(A.col + e);
+    if (j < 0 || j >= i) break;
+    const T l = A.fval[e];
+#pragma unroll
+    for (int d = 0; d < NS; ++d) o[d] = o[d] - l * geto(j, d);
+  }
+  if (blev_i == 0) {
+    const T u = A.fval[__ldg(A.dpos + i)];
+#pragma unroll
+    for (int d = 0; d < NS; ++d) o[d] = o[d] / u;
+  }
+}
+
+template <int NS, typename T, class GetOut>
+__device__ __forceinline__ void ilu_bwd_row_g(const MatT<T> &A, const T (&out_i)[NS], GetOut geto, int i,
+                                              T (&o)[NS]) {
+#pragma unroll
+  for (int d = 0; d < NS; ++d) o[d] = out_i[d];
+  for (int k = A.W - 1; k >= 0; --k) {
+    const size_t e = (size_t)k * A.np + i;
+    const int j = __ldg(A.col + e);
+    if (j <= i) continue;
+    const T u = A.fval[e];
+#pragma unroll
+    for (int d = 0; d < NS; ++d) o[d] = o[d] - u * geto(j, d);
+  }
+  const T u = A.fval[__ldg(A.dpos + i)];
+#pragma unroll
+  for (int d = 0; d < NS; ++d) o[d] = o[d] / u;
 }
 
 // Diagonal preconditioners (Jacobi: 1/|A_ii|; NormDiagonal: 1/norm(column i)),

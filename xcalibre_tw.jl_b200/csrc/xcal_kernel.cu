@@ -15,8 +15,34 @@ enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_KWALL = 2, BC_OMEGAWALL = 3, BC_NUTW
 enum { DIV_LINEAR = 0, DIV_UPWIND = 1 };
 enum { TIME_STEADY = 0, TIME_EULER = 1 };
 enum { GRAD_ORTHOGONAL = 0, GRAD_MIDPOINT = 1 };
-enum { SOLVER_CG = 0, SOLVER_BICGSTAB = 1 };
-enum { PRECON_DILU = 0 };
+enum { SOLVER_CG = 0, SOLVER_BICGSTAB = 1, SOLVER_GMRES = 2 };
+enum { PRECON_DILU = 0, PRECON_ILU0 = 4 };
+
+// Level-scheduled preconditioners (forward and backward sweeps): DILU, ILU(0).
+template <typename T>
+__device__ __forceinline__ bool leveled(const MatT<T> &A) {
+  return A.precon == PRECON_DILU || A.precon == PRECON_ILU0;
+}
+template <typename T>
+__device__ __forceinline__ void lev_setup_row(const MatT<T> &A, int i) {
+  if (A.precon == PRECON_ILU0) ilu_setup_row(A, i);
+  else dilu_setup_row(A, i);
+}
+template <int NS, typename T, class GetOut>
+__device__ __forceinline__ void lev_fwd_row(const MatT<T> &A, const T (&in)[NS], GetOut geto, int i, int blev_i,
+                                            T (&o)[NS]) {
+  if (A.precon == PRECON_ILU0) ilu_fwd_row<NS>(A, in, geto, i, blev_i, o);
+  else dilu_fwd_row<NS>(A, in, geto, i, blev_i, o);
+}
+template <int NS, typename T>
+__device__ __forceinline__ void lev_bwd_row(const MatT<T> &A, const T *out, int i, T (&o)[NS]) {
+  T oi[NS];
+#pragma unroll
+  for (int d = 0; d < NS; ++d) oi[d] = out[(size_t)i * NS + d];
+  auto g = [&](int j, int d) { return out[(size_t)j * NS + d]; };
+  if (A.precon == PRECON_ILU0) ilu_bwd_row_g<NS>(A, oi, g, i, o);
+  else dilu_bwd_row_g<NS>(A, oi, g, i, o);
+}
 
 constexpr int MAXTL = 32;   // tiles per CTA whose warp sums are staged in shared memory
 
@@ -137,6 +163,17 @@ __device__ __forceinline__ bool precon_local(const KParams &P, const MatT<T> &A,
     }
     return true;
   }
+  if (A.precon == PRECON_ILU0) {
+    if (__ldg(P.flev + i) != 0) return false;
+#pragma unroll
+    for (int d = 0; d < NS; ++d) o[d] = in[d];
+    if (__ldg(P.blev + i) == 0) {
+      const T u = A.fval[__ldg(A.dpos + i)];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) o[d] = o[d] / u;
+    }
+    return true;
+  }
   const T di = A.Dinv[i];
 #pragma unroll
   for (int d = 0; d < NS; ++d) o[d] = di * in[d];
@@ -147,7 +184,7 @@ __device__ __forceinline__ bool precon_local(const KParams &P, const MatT<T> &A,
 // row-local part (and, with first_lvl == 2, forward level 1 as well).
 template <typename T>
 __device__ __forceinline__ int precon_tail_phases(const KParams &P, const MatT<T> &A, bool setup, int first_lvl) {
-  if (A.precon != PRECON_DILU) return setup ? 1 : 0;
+  if (!leveled(A)) return setup ? 1 : 0;
   return max(0, P.nfl - first_lvl) + (P.nbl - 1);
 }
 
@@ -162,7 +199,7 @@ __device__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *in, T *out, bool 
     tile_phase<K>(C, true, [&](int i, double (&v)[K]) { red(i, v); });
     return C.sync();
   }
-  if (A.precon != PRECON_DILU) {
+  if (!leveled(A)) {
     if (!setup) return true;
     tile_phase<K>(C, true, [&](int i, double (&v)[K]) {
       diag_precon_setup_row(A, i);
@@ -178,11 +215,11 @@ __device__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *in, T *out, bool 
     const bool last = (++ph == nph);
     tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
       if (__ldg(P.flev + i) == l) {
-        if (setup) dilu_setup_row(A, i);
+        if (setup) lev_setup_row(A, i);
         T iv[NS], o[NS];
 #pragma unroll
         for (int d = 0; d < NS; ++d) iv[d] = in[(size_t)i * NS + d];
-        dilu_fwd_row<NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, __ldg(P.blev + i), o);
+        lev_fwd_row<NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, __ldg(P.blev + i), o);
 #pragma unroll
         for (int d = 0; d < NS; ++d) out[(size_t)i * NS + d] = o[d];
       }
@@ -195,7 +232,7 @@ __device__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *in, T *out, bool 
     tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
       if (__ldg(P.blev + i) == l) {
         T o[NS];
-        dilu_bwd_row<NS>(A, out, i, o);
+        lev_bwd_row<NS>(A, out, i, o);
 #pragma unroll
         for (int d = 0; d < NS; ++d) out[(size_t)i * NS + d] = o[d];
       }
@@ -231,10 +268,10 @@ __device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A64
     r0[d] = (T)(b[d] - y[d]);
     w.x[(size_t)i * NS + d] = T(0);
   }
-  if (A.precon == PRECON_DILU && __ldg(P.flev + i) == 0) dilu_setup_row(A, i);
+  if (leveled(A) && __ldg(P.flev + i) == 0) lev_setup_row(A, i);
   T o[NS];
-  const bool dilu = (A.precon == PRECON_DILU);
-  if (solver == SOLVER_BICGSTAB) {
+  const bool dilu = leveled(A);
+  if (solver != SOLVER_CG) {
 #pragma unroll
     for (int d = 0; d < NS; ++d) w.q[(size_t)i * NS + d] = r0[d];
     if (dilu && precon_local<NS>(P, A, i, r0, o))
@@ -254,7 +291,7 @@ __device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A64
 // accumulated in FP64.
 template <int NS, typename T>
 __device__ bool krylov_start(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, int solver) {
-  if (solver == SOLVER_BICGSTAB) {
+  if (solver != SOLVER_CG) {
     return precon_tail<NS, 2 * NS>(C, A, w.q, w.r[0], true, 1, [&](int i, double (&v)[2 * NS]) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
@@ -466,14 +503,14 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
   }
   const T *z = w.v[0];
   T *zw = w.v[0];
-  const bool dilu = (A.precon == PRECON_DILU);
+  const bool dilu = leveled(A);
   const bool lvl1 = dilu && P.nfl >= 2;
   // With two forward levels every level-1 row has only lower neighbours and
   // every level-0 row only upper ones, so the whole of M^{-1} r fits in the
   // x/r phase: level-0 rows recompute their upper neighbours' forward values
   // (which in turn recompute r of their level-0 neighbours).  Same row
   // functions, same inputs: identical bits, one grid barrier fewer.
-  const bool fuse = dilu && P.nfl == 2 && P.cg_fuse;
+  const bool fuse = A.precon == PRECON_DILU && P.nfl == 2 && P.cg_fuse;
   const int tail = (dilu && !fuse) ? precon_tail_phases(P, A, false, 2) : 0;
   int rc = 0, pc = 0;
   bool first = true;
@@ -546,7 +583,7 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
       } else {
         have = precon_local<NS>(P, A, i, rr, o);
         if (!have && lvl1 && __ldg(P.flev + i) == 1) {
-          dilu_fwd_row<NS>(A, rr, getr, i, __ldg(P.blev + i), o);
+          lev_fwd_row<NS>(A, rr, getr, i, __ldg(P.blev + i), o);
           have = true;
         }
       }
@@ -591,10 +628,226 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
   return true;
 }
 
+// ---------------------------------------------------------------- GMRES
+// Krylov.jl 0.9.5 gmres! with left preconditioner M, N = I, restart = false
+// (the basis grows up to itmax vectors), no reorthogonalisation: modified
+// Gram-Schmidt Arnoldi, QR of the Hessenberg matrix by Givens rotations
+// (SymOrtho, sym_givens), back substitution for y at the end, x = V y.
+// Entry (krylov_start, as for BiCGSTAB): r[0] = M^{-1}(b - A x0), x = 0,
+// partials <b,r>, <r,r>.  Phases of inner iteration k:
+//   P1  V_k = src/div (stored; recomputed for neighbours), t = A V_k,
+//       M^{-1} row-local part
+//   ..  remaining M^{-1} phases, the last reduces h_1 = <V_1, q>
+//   Mi  q -= h_{i-1} V_{i-1}, reduces h_i = <V_i, q>        (i = 2..k)
+//   N   q -= h_k V_k, reduces <q, q>
+// Every CTA's thread 0 then updates its copy of the rotations (c, s, z) and
+// the new column; CTA 0 also stores the column of R for the back substitution.
+__device__ __forceinline__ double sgn1(double a) { return a > 0.0 ? 1.0 : (a < 0.0 ? -1.0 : a); }
+
+__device__ __forceinline__ void sym_givens(double a, double b, double &c, double &s, double &rho) {
+  if (b == 0.0) {
+    c = (a == 0.0) ? 1.0 : sgn1(a);
+    s = 0.0;
+    rho = fabs(a);
+  } else if (a == 0.0) {
+    c = 0.0;
+    s = sgn1(b);
+    rho = fabs(b);
+  } else if (fabs(b) > fabs(a)) {
+    const double t = a / b;
+    s = sgn1(b) / sqrt(1.0 + t * t);
+    c = s * t;
+    rho = b / s;
+  } else {
+    const double t = b / a;
+    c = sgn1(a) / sqrt(1.0 + t * t);
+    s = c * t;
+    rho = a / c;
+  }
+}
+
+template <int NS, typename T>
+__device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg, int (&its)[NS],
+                      double (&rnorm_out)[NS]) {
+  const KParams &P = *C.P;
+  const double BTOL = 1.8189894035458565e-12;   // eps(Float64)^(3/4) = 2^-39
+  double red[2 * NS];
+  final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+  const int G1 = w.gmax + 1;
+  const int kmax = min(cfg.itmax, w.gmax);
+  double *gws = w.gws + (size_t)blockIdx.x * NS * 4 * G1;
+  const size_t rs = (size_t)w.gmax * (w.gmax + 1) / 2;
+  double beta0[NS], rnorm[NS], eps[NS], hbis[NS];
+  unsigned active = 0;
+#pragma unroll
+  for (int d = 0; d < NS; ++d) {
+    its[d] = 0;
+    beta0[d] = sqrt(red[2 * d + 1]);
+    rnorm[d] = beta0[d];
+    hbis[d] = beta0[d];
+    eps[d] = 0.0;
+    if (beta0[d] == 0.0) continue;        // x = 0 is a zero-residual solution
+    eps[d] = cfg.atol + cfg.rtol * rnorm[d];
+    const bool solved = rnorm[d] <= eps[d], tired = 0 >= cfg.itmax;
+    if (!(solved || tired)) active |= 1u << d;
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int d = 0; d < NS; ++d) gws[(size_t)d * 4 * G1 + 2 * G1] = beta0[d];   // z_1 = beta
+  const unsigned ran = active;
+  const T *r0 = w.r[0];
+  T *qb[2] = {w.v[0], w.v[1]};
+  const size_t nv = (size_t)P.n * NS;
+  const int tail = precon_tail_phases(P, A, false, 1);
+  int k = 0;
+  while (active) {
+    ++k;
+    const T *src = (k == 1) ? r0 : qb[(k - 1) & 1];
+    T *qn = qb[k & 1];
+    T *Vk = w.V + (size_t)(k - 1) * nv;
+    double div[NS];
+#pragma unroll
+    for (int d = 0; d < NS; ++d) div[d] = (k == 1) ? beta0[d] : hbis[d];
+    auto getv = [&](int j, int d) -> T { return (T)((double)src[(size_t)j * NS + d] / div[d]); };
+    // P1: V_k, t = A V_k, M^{-1} row-local part
+    tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
+      T y[NS], o[NS], vk[NS];
+      spmv_row<NS>(A, i, getv, y);
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        vk[d] = getv(i, d);
+        Vk[(size_t)i * NS + d] = vk[d];
+        w.t[(size_t)i * NS + d] = y[d];
+      }
+      if (precon_local<NS>(P, A, i, y, o))
+#pragma unroll
+        for (int d = 0; d < NS; ++d) qn[(size_t)i * NS + d] = o[d];
+      if (tail == 0)
+#pragma unroll
+        for (int d = 0; d < NS; ++d) {
+          const double v1 = (k == 1) ? (double)vk[d] : (double)w.V[(size_t)i * NS + d];
+          v[d] = v1 * (double)o[d];
+        }
+    });
+    if (!C.sync()) return false;
+    if (!precon_tail<NS, NS>(C, A, (const T *)w.t, qn, false, 1, [&](int i, double (&v)[NS]) {
+#pragma unroll
+          for (int d = 0; d < NS; ++d)
+            v[d] = (double)w.V[(size_t)i * NS + d] * (double)qn[(size_t)i * NS + d];
+        }))
+      return false;
+    double h[NS];
+    final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, h);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int d = 0; d < NS; ++d) gws[(size_t)d * 4 * G1 + 3 * G1] = h[d];
+    // modified Gram-Schmidt against V_2..V_k, each dot after the previous update
+    for (int m = 2; m <= k + 1; ++m) {
+      const T *Vp = w.V + (size_t)(m - 2) * nv;
+      const T *Vm = w.V + (size_t)(m - 1) * nv;
+      const bool norm = (m == k + 1);
+      tile_phase<NS>(C, true, [&](int i, double (&v)[NS]) {
+#pragma unroll
+        for (int d = 0; d < NS; ++d) {
+          const size_t q = (size_t)i * NS + d;
+          const T qv = (T)((double)qn[q] + (-h[d]) * (double)Vp[q]);
+          qn[q] = qv;
+          v[d] = norm ? (double)qv * (double)qv : (double)Vm[q] * (double)qv;
+        }
+      });
+      if (!C.sync()) return false;
+      final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, h);
+      if (!norm && threadIdx.x == 0)
+#pragma unroll
+        for (int d = 0; d < NS; ++d) gws[(size_t)d * 4 * G1 + 3 * G1 + (m - 1)] = h[d];
+    }
+#pragma unroll
+    for (int d = 0; d < NS; ++d) hbis[d] = sqrt(h[d]);
+    // Givens: previous rotations on the new column, then the new rotation
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        if (!(active & (1u << d))) continue;
+        double *cs = gws + (size_t)d * 4 * G1, *sn = cs + G1, *zz = sn + G1, *col = zz + G1;
+        for (int i = 0; i < k - 1; ++i) {
+          const double tmp = cs[i] * col[i] + sn[i] * col[i + 1];
+          col[i + 1] = sn[i] * col[i] - cs[i] * col[i + 1];
+          col[i] = tmp;
+        }
+        double c_, s_, rho;
+        sym_givens(col[k - 1], hbis[d], c_, s_, rho);
+        cs[k - 1] = c_;
+        sn[k - 1] = s_;
+        col[k - 1] = rho;
+        const double zeta = s_ * zz[k - 1];
+        zz[k - 1] = c_ * zz[k - 1];
+        zz[k] = zeta;
+        C.sm_out[d] = fabs(zeta);
+        if (blockIdx.x == 0) {
+          double *Rc = w.gR + (size_t)d * rs + (size_t)(k - 1) * k / 2;
+          for (int i = 0; i < k; ++i) Rc[i] = col[i];
+        }
+      }
+    }
+    __syncthreads();
+    unsigned cont = 0;
+#pragma unroll
+    for (int d = 0; d < NS; ++d) {
+      if (!(active & (1u << d))) continue;
+      rnorm[d] = C.sm_out[d];
+      its[d] = k;
+      const bool mach = (rnorm[d] + 1.0 <= 1.0);
+      const bool solved = (rnorm[d] <= eps[d]) || mach;
+      const bool breakdown = hbis[d] <= BTOL;
+      const bool tired = k >= kmax;
+      if (!(solved || tired || breakdown)) cont |= 1u << d;
+    }
+    __syncthreads();
+    active = cont;
+  }
+  if (ran) {
+    // R complete (CTA 0's stores) after this barrier; y by back substitution
+    if (!C.sync()) return false;
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        if (!(ran & (1u << d))) continue;
+        const int kd = its[d];
+        double *zz = gws + (size_t)d * 4 * G1 + 2 * G1, *y = zz + G1;
+        const double *R = w.gR + (size_t)d * rs;
+        for (int i = 0; i < kd; ++i) y[i] = zz[i];
+        for (int i = kd - 1; i >= 0; --i) {
+          double yi = y[i];
+          for (int j = kd - 1; j >= i + 1; --j) yi = yi - R[(size_t)j * (j + 1) / 2 + i] * y[j];
+          const double rii = R[(size_t)i * (i + 1) / 2 + i];
+          y[i] = (fabs(rii) <= BTOL) ? 0.0 : yi / rii;
+        }
+      }
+    }
+    __syncthreads();
+    tile_each(P, [&](int i) {
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        if (!(ran & (1u << d))) continue;
+        const double *y = gws + (size_t)d * 4 * G1 + 3 * G1;
+        const size_t q = (size_t)i * NS + d;
+        double acc = (double)w.x[q];
+        for (int m = 0; m < its[d]; ++m) acc = acc + y[m] * (double)w.V[(size_t)m * nv + q];
+        w.x[q] = (T)acc;
+      }
+    });
+    if (!C.sync()) return false;
+  }
+#pragma unroll
+  for (int d = 0; d < NS; ++d) rnorm_out[d] = rnorm[d];
+  return true;
+}
+
 template <int NS, typename T>
 __device__ bool krylov(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, const KCfg &cfg,
                        int solver, int (&its)[NS], double (&rn)[NS]) {
   if (solver == SOLVER_BICGSTAB) return bicgstab<NS, T>(C, A, w, b, cfg, its, rn);
+  if (solver == SOLVER_GMRES) return gmres<NS, T>(C, A, w, cfg, its, rn);
   return cg<NS, T>(C, A, w, cfg, its, rn);
 }
 

@@ -24,8 +24,8 @@ BC_DIRICHLET, BC_NEUMANN, BC_KWALL, BC_OMEGAWALL, BC_NUTWALL = 0, 1, 2, 3, 4
 TIME_STEADY, TIME_EULER = 0, 1
 DIV_LINEAR, DIV_UPWIND = 0, 1
 GRAD_ORTHOGONAL, GRAD_MIDPOINT = 0, 1
-SOLVER_CG, SOLVER_BICGSTAB = 0, 1
-PRECON_DILU, PRECON_JACOBI, PRECON_NORMDIAG, PRECON_NONE = 0, 1, 2, 3
+SOLVER_CG, SOLVER_BICGSTAB, SOLVER_GMRES = 0, 1, 2
+PRECON_DILU, PRECON_JACOBI, PRECON_NORMDIAG, PRECON_NONE, PRECON_ILU0 = 0, 1, 2, 3, 4
 MODEL_LAMINAR, MODEL_KOMEGA = 0, 1
 RENUMBER_NONE, RENUMBER_RCM, RENUMBER_COLOR = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1

@@ -81,8 +81,7 @@ class CgSolver: code = _abi.SOLVER_CG
 class BicgstabSolver: code = _abi.SOLVER_BICGSTAB
 
 
-class GmresSolver:
-    code = None   # GMRES is not part of the device path
+class GmresSolver: code = _abi.SOLVER_GMRES
 
 
 class DILU: code = _abi.PRECON_DILU
@@ -90,8 +89,7 @@ class Jacobi: code = _abi.PRECON_JACOBI
 class NormDiagonal: code = _abi.PRECON_NORMDIAG
 
 
-class ILU0:
-    code = None
+class ILU0: code = _abi.PRECON_ILU0
 
 
 class LDL:
