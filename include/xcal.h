@@ -103,6 +103,12 @@ typedef struct {
   const int64_t *patch_ptr;         /* [npatches+1] 0-based offsets into patch_faces/cells */
   const int64_t *patch_faces;       /* 1-based boundary.facesID, concatenated */
   const int64_t *patch_cells;       /* 1-based boundary.cellsID, concatenated */
+  /* Optional (nnodes = 0: absent): mesh.nodes and mesh.cell_nodes, needed
+   * only by the VTK writer. */
+  int64_t nnodes;
+  const double *node_coords;        /* [nnodes*3] */
+  const int64_t *cell_nodes_ptr;    /* [ncells+1] 1-based start of nodes_range; ptr[n]=total+1 */
+  const int64_t *cell_nodes;        /* [total] 1-based node ids (mesh.cell_nodes) */
 } xcal_mesh_desc;
 
 /* ------------------------------------------------------------ case config */
@@ -245,6 +251,29 @@ int xcal_residual(xcal_ctx ctx, int64_t n, const int32_t *row_ptr, const int32_t
  * context's stream; calls that overlap on the GPU share the array and race. */
 int xcal_residual_noalloc(xcal_ctx ctx, int64_t n, const int32_t *d_row_ptr, const int32_t *d_col,
                           const double *d_val, const double *d_x, const double *d_b, double *d_R);
+
+/* ------------------------------------------------------- post-processing
+ * write_vtk(name, mesh, ("label", field)...) (src/VTK/VTK_writer.jl:22-116):
+ * legacy ASCII unstructured grid "<name>.vtk" with POINTS, CELLS (0-based
+ * node ids), CELL_TYPES (3 nodes: 5, 4 nodes: 9, more: 7) and CELL_DATA.
+ * ncomp[f] = 1 writes SCALARS (data[f] = ncells values), 3 writes VECTORS
+ * (data[f] = x, y, z arrays of ncells each, concatenated).  Numbers are
+ * written in shortest round-trip form.  Needs the mesh's nodes. */
+int xcal_vtk_write(const char *name, const xcal_mesh_desc *mesh, int32_t nfields, const char *const *labels,
+                   const int32_t *ncomp, const double *const *data);
+/* model2vtk(model, name) (VTK_writer.jl:3-20): the context's U and p (and k,
+ * omega, nut for k-omega) in the caller's cell order. */
+int xcal_model2vtk(xcal_ctx ctx, const char *name);
+/* wall_shear_stress(patch, model) (src/Postprocess/Postprocess_forces.jl:61-94
+ * with surface_normal_gradient, src/Calculate/Calculate_5_surface_normal_gradient.jl:20-37):
+ * per face of the patch (0-based patch index), tau = (nu + nut_c) * Up/delta,
+ * Up = (U_c - Uw) - ((U_c - Uw).n) n, Uw the patch's Dirichlet U value;
+ * tau and pos (face centres) are [3*count] (x,y,z per face); cap = room. */
+int xcal_wall_shear_stress(xcal_ctx ctx, int32_t patch, double *tau, double *pos, int64_t cap, int64_t *count);
+/* pressure_force(patch, p, rho) and viscous_force(patch, U, rho, nu, nut)
+ * (Postprocess_forces.jl:5-59), with the context's fields and viscosity. */
+int xcal_pressure_force(xcal_ctx ctx, int32_t patch, double rho, double F[3]);
+int xcal_viscous_force(xcal_ctx ctx, int32_t patch, double rho, double F[3]);
 
 /* ------------------------------------------------------------- serving
  * A stream of independent cases on one GPU (no reference counterpart: the

@@ -70,6 +70,13 @@ void HostMesh::prepare_export() {
   for (size_t k = 0; k < pfaces.size(); ++k) { x_pf[k] = pfaces[k] + 1; x_pc[k] = pcells[k] + 1; }
   names.clear();
   for (auto &s : pname) { names += s; names += "\n"; }
+  x_cnp.clear(); x_cnode.clear();
+  if (!cn_ptr.empty()) {
+    x_cnp.resize(cn_ptr.size());
+    for (size_t c = 0; c < cn_ptr.size(); ++c) x_cnp[c] = cn_ptr[c] + 1;
+    x_cnode.resize(cn.size());
+    for (size_t k = 0; k < cn.size(); ++k) x_cnode[k] = cn[k] + 1;
+  }
 }
 
 int build_unv(const char *path, double scale, HostMesh &M, std::string &err) {
@@ -290,6 +297,16 @@ int build_unv(const char *path, double scale, HostMesh &M, std::string &err) {
   }
   M.nc = nc; M.nf = nf; M.nbf = nbf; M.dim = 2; M.nnodes = np;
   M.o1 = o1; M.o2 = o2;
+  // mesh.nodes and mesh.cell_nodes (element vertex order), for VTK output
+  M.nodes.resize(3 * (size_t)np);
+  for (int64_t i = 0; i < np; ++i) { M.nodes[3 * i] = pts[i].x; M.nodes[3 * i + 1] = pts[i].y; M.nodes[3 * i + 2] = pts[i].z; }
+  M.cn_ptr.assign(nc + 1, 0);
+  M.cn.clear();
+  for (int64_t c = 0; c < nc; ++c) {
+    const El &e = els[first + c];
+    for (int k = 0; k < e.nv; ++k) M.cn.push_back(e.v[k] - 1);
+    M.cn_ptr[c + 1] = (int64_t)M.cn.size();
+  }
   M.prepare_export();
   return XCAL_OK;
 }
@@ -352,6 +369,21 @@ int mesh_from_desc(const xcal_mesh_desc *d, HostMesh &M, std::string &err) {
     M.pptr[p + 1] = (int64_t)M.pfaces.size();
   }
   for (int64_t c = 0; c < nc; ++c) if (!(M.cvol[c] > 0.0)) { err = "non-positive cell volume"; return XCAL_ERR_MESH; }
+  M.nodes.clear(); M.cn_ptr.clear(); M.cn.clear(); M.nnodes = 0;
+  if (d->nnodes > 0) {
+    if (!d->node_coords || !d->cell_nodes_ptr || !d->cell_nodes) { err = "null node arrays"; return XCAL_ERR_ARG; }
+    M.nnodes = d->nnodes;
+    M.nodes.assign(d->node_coords, d->node_coords + 3 * d->nnodes);
+    M.cn_ptr.resize(nc + 1);
+    for (int64_t c = 0; c <= nc; ++c) M.cn_ptr[c] = d->cell_nodes_ptr[c] - 1;
+    if (M.cn_ptr[0] != 0) { err = "cell_nodes_ptr must start at 1"; return XCAL_ERR_MESH; }
+    for (int64_t c = 0; c < nc; ++c) if (M.cn_ptr[c + 1] < M.cn_ptr[c]) { err = "cell_nodes_ptr not monotone"; return XCAL_ERR_MESH; }
+    M.cn.resize(M.cn_ptr[nc]);
+    for (int64_t k = 0; k < M.cn_ptr[nc]; ++k) {
+      M.cn[k] = d->cell_nodes[k] - 1;
+      if (M.cn[k] < 0 || M.cn[k] >= d->nnodes) { err = "cell node id out of range"; return XCAL_ERR_MESH; }
+    }
+  }
   M.prepare_export();
   return XCAL_OK;
 }
@@ -474,6 +506,15 @@ void apply_perm(const HostMesh &in, const std::vector<int64_t> &perm, bool reord
     int64_t oc = inv[c];
     for (int d = 0; d < 3; ++d) out.cc[3 * c + d] = in.cc[3 * oc + d];
     out.cvol[c] = in.cvol[oc];
+  }
+  out.nodes = in.nodes;
+  if (!in.cn_ptr.empty()) {
+    out.cn_ptr.assign(nc + 1, 0);
+    for (int64_t c = 0; c < nc; ++c) {
+      const int64_t oc = inv[c];
+      out.cn.insert(out.cn.end(), in.cn.begin() + in.cn_ptr[oc], in.cn.begin() + in.cn_ptr[oc + 1]);
+      out.cn_ptr[c + 1] = (int64_t)out.cn.size();
+    }
   }
   out.o1.resize(nf); out.o2.resize(nf);
   out.fc.resize(3 * nf); out.fn.resize(3 * nf); out.fe.resize(3 * nf);

@@ -18,8 +18,10 @@ struct HostMesh {
   std::vector<double> fc, fn, fe, farea, fdelta, fweight;   // fc/fn/fe [3*nf]
   std::vector<std::string> pname;
   std::vector<int64_t> pptr, pfaces, pcells;       // concatenated patches
+  std::vector<double> nodes;                       // [3*nnodes] (optional: VTK output)
+  std::vector<int64_t> cn_ptr, cn;                 // cell node lists, 0-based (optional)
   // 1-based export copies (xcal_hmesh_desc)
-  std::vector<int64_t> x_cfp, x_cf, x_cn, x_own, x_pf, x_pc;
+  std::vector<int64_t> x_cfp, x_cf, x_cn, x_own, x_pf, x_pc, x_cnp, x_cnode;
   std::string names;
   void prepare_export();
 };

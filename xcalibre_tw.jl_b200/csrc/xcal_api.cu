@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -65,6 +66,7 @@ struct xcal_ctx_s {
   double *pin = nullptr;       // pinned staging [n*3]
   size_t pin_n = 0;
   std::vector<BcEntry> tabU, tabP;
+  std::vector<xcal_bc> bcU_host;   // the case's U conditions (post-processing)
 };
 
 struct xcal_hmesh_s {
@@ -259,9 +261,15 @@ int xcal_hmesh_counts(xcal_hmesh h, int64_t *c) {
   return XCAL_OK;
 }
 
+static void fill_desc(const HostMesh &M, xcal_mesh_desc *d);
+
 int xcal_hmesh_desc(xcal_hmesh h, xcal_mesh_desc *d) {
   if (!h || !d) return XCAL_ERR_ARG;
-  HostMesh &M = h->M;
+  fill_desc(h->M, d);
+  return XCAL_OK;
+}
+
+static void fill_desc(const HostMesh &M, xcal_mesh_desc *d) {
   d->ncells = M.nc; d->nfaces = M.nf; d->nbfaces = M.nbf; d->dim = M.dim;
   d->cell_centre = M.cc.data(); d->cell_volume = M.cvol.data();
   d->cell_faces_ptr = M.x_cfp.data(); d->cell_faces = M.x_cf.data(); d->cell_neighbours = M.x_cn.data();
@@ -270,7 +278,10 @@ int xcal_hmesh_desc(xcal_hmesh h, xcal_mesh_desc *d) {
   d->face_delta = M.fdelta.data(); d->face_weight = M.fweight.data();
   d->npatches = (int64_t)M.pname.size(); d->patch_ptr = M.pptr.data(); d->patch_faces = M.x_pf.data();
   d->patch_cells = M.x_pc.data();
-  return XCAL_OK;
+  d->nnodes = M.cn_ptr.empty() ? 0 : M.nnodes;
+  d->node_coords = M.nodes.empty() ? nullptr : M.nodes.data();
+  d->cell_nodes_ptr = M.x_cnp.empty() ? nullptr : M.x_cnp.data();
+  d->cell_nodes = M.x_cnode.empty() ? nullptr : M.x_cnode.data();
 }
 
 int xcal_hmesh_patch_names(xcal_hmesh h, char *buf, size_t n) {
@@ -510,6 +521,7 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   int n = c->prep.n, nf = c->prep.nf, NS = c->ns;
   size_t nnz = (size_t)c->prep.W * c->prep.np;
   TRY(build_bc(c, B, cfg->bc_U, cfg->nbc_U, h.bcU, c->tabU, true, "U"));
+  c->bcU_host.assign(cfg->bc_U, cfg->bc_U + cfg->nbc_U);
   TRY(build_bc(c, B, cfg->bc_p, cfg->nbc_p, h.bcP, c->tabP, false, "p"));
   h.model = cfg->model;
   if (turb) {
@@ -932,6 +944,190 @@ int xcal_residual_noalloc(xcal_ctx c, int64_t n64, const int32_t *d_row_ptr, con
   CUDA_TRY(c, noalloc_scratch(c->device, &scratch));
   CUDA_TRY(c, launch_residual((int)n64, d_row_ptr, d_col, d_val, d_x, d_b, scratch, d_R, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return XCAL_OK;
+}
+
+
+// ------------------------------------------------------- post-processing
+static void put_num(std::string &out, double v) {
+  char buf[64];
+  auto r = std::to_chars(buf, buf + sizeof(buf), v);
+  out.append(buf, r.ptr);
+}
+
+int xcal_vtk_write(const char *name, const xcal_mesh_desc *d, int32_t nfields, const char *const *labels,
+                   const int32_t *ncomp, const double *const *data) {
+  if (!name || !d || nfields < 0 || (nfields > 0 && (!labels || !ncomp || !data))) return XCAL_ERR_ARG;
+  if (d->nnodes <= 0 || !d->node_coords || !d->cell_nodes_ptr || !d->cell_nodes) return XCAL_ERR_UNSUPPORTED;
+  for (int f = 0; f < nfields; ++f)
+    if (!labels[f] || !data[f] || (ncomp[f] != 1 && ncomp[f] != 3)) return XCAL_ERR_ARG;
+  const int64_t nc = d->ncells, nn = d->nnodes;
+  std::string out;
+  out.reserve((size_t)(nn * 60 + nc * 40 * (2 + nfields)));
+  out += "# vtk DataFile Version 3.0\njCFD simulation data\nASCII\nDATASET UNSTRUCTURED_GRID\n";
+  out += "POINTS " + std::to_string(nn) + " double\n";
+  for (int64_t i = 0; i < nn; ++i) {
+    put_num(out, d->node_coords[3 * i]); out += ' ';
+    put_num(out, d->node_coords[3 * i + 1]); out += ' ';
+    put_num(out, d->node_coords[3 * i + 2]); out += '\n';
+  }
+  const int64_t total = d->cell_nodes_ptr[nc] - d->cell_nodes_ptr[0];
+  out += "CELLS " + std::to_string(nc) + " " + std::to_string(total + nc) + "\n";
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t b = d->cell_nodes_ptr[c] - 1, e = d->cell_nodes_ptr[c + 1] - 1;
+    out += std::to_string(e - b) + " ";          // println(io, nNodes, " ", nodes): nodes = " id0 id1 ..."
+    for (int64_t k = b; k < e; ++k) {
+      if (d->cell_nodes[k] < 1 || d->cell_nodes[k] > nn) return XCAL_ERR_MESH;
+      out += ' ';
+      out += std::to_string(d->cell_nodes[k] - 1);
+    }
+    out += '\n';
+  }
+  out += "CELL_TYPES " + std::to_string(nc) + "\n";
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t k = d->cell_nodes_ptr[c + 1] - d->cell_nodes_ptr[c];
+    out += (k == 3) ? "5\n" : (k == 4) ? "9\n" : "7\n";
+  }
+  out += "CELL_DATA " + std::to_string(nc) + "\n";
+  for (int f = 0; f < nfields; ++f) {
+    const double *v = data[f];
+    if (ncomp[f] == 1) {
+      out += std::string("SCALARS ") + labels[f] + " double 1\nLOOKUP_TABLE CellColors\n";
+      for (int64_t c = 0; c < nc; ++c) { put_num(out, v[c]); out += '\n'; }
+    } else {
+      out += std::string("VECTORS ") + labels[f] + " double\n";
+      for (int64_t c = 0; c < nc; ++c) {
+        put_num(out, v[c]); out += ' ';
+        put_num(out, v[nc + c]); out += ' ';
+        put_num(out, v[2 * nc + c]); out += '\n';
+      }
+    }
+  }
+  FILE *fp = fopen((std::string(name) + ".vtk").c_str(), "wb");
+  if (!fp) return XCAL_ERR_IO;
+  const size_t w = fwrite(out.data(), 1, out.size(), fp);
+  const int cl = fclose(fp);
+  return (w == out.size() && cl == 0) ? XCAL_OK : XCAL_ERR_IO;
+}
+
+static int host_fields(xcal_ctx c, std::vector<double> &U, std::vector<double> &p, std::vector<double> *nut) {
+  const int64_t n = c->user.nc;
+  U.assign(3 * (size_t)n, 0.0);
+  p.assign((size_t)n, 0.0);
+  for (int d = 0; d < 3; ++d) TRY(xcal_field_get(c, XCAL_FIELD_UX + d, U.data() + (size_t)d * n, n));
+  TRY(xcal_field_get(c, XCAL_FIELD_P, p.data(), n));
+  if (nut) {
+    nut->assign((size_t)n, 0.0);
+    if (c->hp.model == XCAL_MODEL_KOMEGA) TRY(xcal_field_get(c, XCAL_FIELD_NUT, nut->data(), n));
+  }
+  return XCAL_OK;
+}
+
+int xcal_model2vtk(xcal_ctx c, const char *name) {
+  if (!c || !name) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_model2vtk before xcal_case_setup");
+  std::vector<double> U, p, k, w, nut;
+  TRY(host_fields(c, U, p, nullptr));
+  std::vector<const char *> labels = {"U", "p"};
+  std::vector<int32_t> nco = {3, 1};
+  std::vector<const double *> data = {U.data(), p.data()};
+  if (c->hp.model == XCAL_MODEL_KOMEGA) {
+    const int64_t n = c->user.nc;
+    k.resize(n); w.resize(n); nut.resize(n);
+    TRY(xcal_field_get(c, XCAL_FIELD_K, k.data(), n));
+    TRY(xcal_field_get(c, XCAL_FIELD_OMEGA, w.data(), n));
+    TRY(xcal_field_get(c, XCAL_FIELD_NUT, nut.data(), n));
+    labels.insert(labels.end(), {"k", "omega", "nut"});
+    nco.insert(nco.end(), {1, 1, 1});
+    data.insert(data.end(), {k.data(), w.data(), nut.data()});
+  }
+  xcal_mesh_desc d;
+  fill_desc(c->user, &d);
+  const int st = xcal_vtk_write(name, &d, (int32_t)labels.size(), labels.data(), nco.data(), data.data());
+  if (st == XCAL_ERR_UNSUPPORTED) return fail(c, st, "mesh has no node coordinates (xcal_mesh_desc.nnodes = 0)");
+  if (st) return fail(c, st, "VTK write failed");
+  return XCAL_OK;
+}
+
+// Dirichlet value of U on a patch (the reference looks it up in U.BCs)
+static int patch_Uw(xcal_ctx c, int32_t patch, double Uw[3]) {
+  for (const xcal_bc &b : c->bcU_host)
+    if (b.patch == patch) {
+      if (b.type != XCAL_BC_DIRICHLET) return fail(c, XCAL_ERR_ARG, "patch has no Dirichlet U condition");
+      for (int d = 0; d < 3; ++d) Uw[d] = b.value[d];
+      return XCAL_OK;
+    }
+  return fail(c, XCAL_ERR_ARG, "patch has no U condition");
+}
+
+int xcal_wall_shear_stress(xcal_ctx c, int32_t patch, double *tau, double *pos, int64_t cap, int64_t *count) {
+  if (!c || !count) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_wall_shear_stress before xcal_case_setup");
+  const HostMesh &M = c->user;
+  if (patch < 0 || patch >= (int32_t)M.pname.size()) return fail(c, XCAL_ERR_ARG, "patch index out of range");
+  const int64_t a = M.pptr[patch], b = M.pptr[patch + 1];
+  *count = b - a;
+  if (!tau || !pos || cap < b - a) return fail(c, XCAL_ERR_ARG, "output arrays smaller than the patch");
+  double Uw[3];
+  TRY(patch_Uw(c, patch, Uw));
+  std::vector<double> U, p, nut;
+  TRY(host_fields(c, U, p, &nut));
+  const int64_t n = M.nc;
+  for (int64_t i = a; i < b; ++i) {
+    const int64_t f = M.pfaces[i], cell = M.pcells[i];
+    const double *nrm = &M.fn[3 * f];
+    double ud[3], up[3];
+    for (int d = 0; d < 3; ++d) ud[d] = U[(size_t)d * n + cell] - Uw[d];
+    const double dn = (ud[0] * nrm[0] + ud[1] * nrm[1]) + ud[2] * nrm[2];
+    for (int d = 0; d < 3; ++d) up[d] = ud[d] - dn * nrm[d];
+    const double nueff = c->hp.nu + nut[cell];
+    for (int d = 0; d < 3; ++d) {
+      tau[3 * (i - a) + d] = (up[d] / M.fdelta[f]) * nueff;
+      pos[3 * (i - a) + d] = M.fc[3 * f + d];
+    }
+  }
+  return XCAL_OK;
+}
+
+int xcal_pressure_force(xcal_ctx c, int32_t patch, double rho, double F[3]) {
+  if (!c || !F) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_pressure_force before xcal_case_setup");
+  const HostMesh &M = c->user;
+  if (patch < 0 || patch >= (int32_t)M.pname.size()) return fail(c, XCAL_ERR_ARG, "patch index out of range");
+  std::vector<double> U, p;
+  TRY(host_fields(c, U, p, nullptr));
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = M.pptr[patch]; i < M.pptr[patch + 1]; ++i) {
+    const int64_t f = M.pfaces[i], cell = M.pcells[i];
+    for (int d = 0; d < 3; ++d) s[d] += p[cell] * (M.farea[f] * M.fn[3 * f + d]);
+  }
+  for (int d = 0; d < 3; ++d) F[d] = rho * s[d];
+  return XCAL_OK;
+}
+
+int xcal_viscous_force(xcal_ctx c, int32_t patch, double rho, double F[3]) {
+  if (!c || !F) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_viscous_force before xcal_case_setup");
+  const HostMesh &M = c->user;
+  if (patch < 0 || patch >= (int32_t)M.pname.size()) return fail(c, XCAL_ERR_ARG, "patch index out of range");
+  double Uw[3];
+  TRY(patch_Uw(c, patch, Uw));
+  std::vector<double> U, p, nut;
+  TRY(host_fields(c, U, p, &nut));
+  const int64_t n = M.nc;
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = M.pptr[patch]; i < M.pptr[patch + 1]; ++i) {
+    const int64_t f = M.pfaces[i], cell = M.pcells[i];
+    const double *nrm = &M.fn[3 * f];
+    double ud[3];
+    for (int d = 0; d < 3; ++d) ud[d] = U[(size_t)d * n + cell] - Uw[d];
+    const double dn = (ud[0] * nrm[0] + ud[1] * nrm[1]) + ud[2] * nrm[2];
+    for (int d = 0; d < 3; ++d) {
+      const double g = (ud[d] - dn * nrm[d]) / M.fdelta[f];
+      s[d] += g * M.farea[f] * (c->hp.nu + nut[cell]);
+    }
+  }
+  for (int d = 0; d < 3; ++d) F[d] = rho * s[d];
   return XCAL_OK;
 }
 

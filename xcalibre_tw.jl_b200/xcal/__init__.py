@@ -6,5 +6,5 @@ from .api import (  # noqa: F401
     ILU0, Jacobi, KOmega, KWallFunction, LDL, Laminar, Linear, Midpoint, Neumann, NormDiagonal,
     NutWallFunction, OmegaWallFunction, Orthogonal, RANS, ScalarField, Server, Solver, Steady, Upwind,
     VectorField, assign, build_mesh, initialise, isturbulent, make_case, piso, set_runtime,
-    set_schemes, set_solver, simple, update_mesh_format)
+    set_schemes, set_solver, simple, update_mesh_format, write_vtk, model2vtk)
 from .mesh import Mesh2  # noqa: F401

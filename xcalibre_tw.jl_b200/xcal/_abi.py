@@ -48,6 +48,7 @@ class MeshDesc(C.Structure):
         ("face_area", P_d), ("face_delta", P_d), ("face_weight", P_d),
         ("npatches", C.c_int64), ("patch_ptr", P_i64), ("patch_faces", P_i64),
         ("patch_cells", P_i64),
+        ("nnodes", C.c_int64), ("node_coords", P_d), ("cell_nodes_ptr", P_i64), ("cell_nodes", P_i64),
     ]
 
 
@@ -148,6 +149,12 @@ SIGNATURES = {
     "xcal_residual_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p]),
     "xcal_ctx_set_tolerance": (C.c_int, [C.c_void_p, C.c_double]),
+    "xcal_vtk_write": (C.c_int, [C.c_char_p, C.POINTER(MeshDesc), C.c_int32, C.POINTER(C.c_char_p), P_i32,
+                                 C.POINTER(P_d)]),
+    "xcal_model2vtk": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "xcal_wall_shear_stress": (C.c_int, [C.c_void_p, C.c_int32, P_d, P_d, C.c_int64, P_i64]),
+    "xcal_pressure_force": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, P_d]),
+    "xcal_viscous_force": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, P_d]),
     "xcal_serve_create": (C.c_int, [C.c_int, C.POINTER(ServeCfg), C.POINTER(C.c_void_p)]),
     "xcal_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(Case), P_d, P_d,
                                     P_i64]),

@@ -345,6 +345,34 @@ class Solver:
     def setup(self, case):
         _abi.check(self.lib.xcal_case_setup(self.ctx, C.byref(case)), self.ctx, "xcal_case_setup")
 
+    # --- post-processing (src/VTK/VTK_writer.jl, src/Postprocess/Postprocess_forces.jl)
+    def model2vtk(self, name):
+        """model2vtk: '<name>.vtk' with this context's U, p (k, omega, nut)."""
+        _abi.check(self.lib.xcal_model2vtk(self.ctx, str(name).encode()), self.ctx, "xcal_model2vtk")
+
+    def wall_shear_stress(self, patch):
+        """wall_shear_stress(:patch, model) -> (tau [nfaces,3], face centres [nfaces,3])."""
+        pid = self.mesh.boundary_index(patch) - 1
+        m = int(self.mesh.patch_ptr[pid + 1] - self.mesh.patch_ptr[pid])
+        tau = np.zeros(3 * m)
+        pos = np.zeros(3 * m)
+        cnt = np.zeros(1, dtype=np.int64)
+        _abi.check(self.lib.xcal_wall_shear_stress(self.ctx, pid, _abi.dptr(tau), _abi.dptr(pos), m,
+                                                   _abi.i64ptr(cnt)), self.ctx, "xcal_wall_shear_stress")
+        return tau.reshape(m, 3), pos.reshape(m, 3)
+
+    def pressure_force(self, patch, rho):
+        F = np.zeros(3)
+        _abi.check(self.lib.xcal_pressure_force(self.ctx, self.mesh.boundary_index(patch) - 1, float(rho),
+                                                _abi.dptr(F)), self.ctx, "xcal_pressure_force")
+        return F
+
+    def viscous_force(self, patch, rho):
+        F = np.zeros(3)
+        _abi.check(self.lib.xcal_viscous_force(self.ctx, self.mesh.boundary_index(patch) - 1, float(rho),
+                                               _abi.dptr(F)), self.ctx, "xcal_viscous_force")
+        return F
+
     def set_tolerance(self, tol):
         """SIMPLE stop tolerance (1e-7 as in the reference unless changed)."""
         _abi.check(self.lib.xcal_ctx_set_tolerance(self.ctx, float(tol)), self.ctx, "xcal_ctx_set_tolerance")
@@ -473,6 +501,44 @@ def piso(model, config, resume=True, pref=None, renumber=_abi.RENUMBER_COLOR, de
          precision=_abi.PREC_FP64):
     """piso!(model, config; resume, pref) -> (R_ux, R_uy, R_p); fields updated in place."""
     return _run(model, config, pref, True, renumber, device, precision)
+
+
+def write_vtk(name, mesh, *args):
+    """write_vtk(name, mesh, ("label", field)...) (src/VTK/VTK_writer.jl:22-116):
+    '<name>.vtk' with the given ScalarField/VectorField cell values.  Needs the
+    mesh's nodes (meshes built from UNV files carry them)."""
+    lib = _abi.load()
+    labels, nco, data, keep = [], [], [], []
+    for label, field in args:
+        if isinstance(field, VectorField):
+            arr = np.ascontiguousarray(np.concatenate([field.x.values, field.y.values, field.z.values]),
+                                       dtype=np.float64)
+            nco.append(3)
+        elif isinstance(field, ScalarField):
+            arr = np.ascontiguousarray(field.values, dtype=np.float64)
+            nco.append(1)
+        else:
+            raise TypeError('Input data should be a ScalarField or VectorField e.g. ("U", U)')
+        keep.append(arr)
+        labels.append(str(label).encode())
+        data.append(_abi.dptr(arr))
+    n = len(labels)
+    lab = (C.c_char_p * max(n, 1))(*labels)
+    nc = np.array(nco or [0], dtype=np.int32)
+    dat = (_abi.P_d * max(n, 1))(*data)
+    st = lib.xcal_vtk_write(str(name).encode(), C.byref(mesh.desc()), n, lab, _abi.i32ptr(nc), dat)
+    if st == -9:
+        raise _abi.XcalError("write_vtk: the mesh has no node coordinates")
+    _abi.check(st, None, "xcal_vtk_write")
+
+
+def model2vtk(model, name):
+    """model2vtk(model, name) (VTK_writer.jl:3-20)."""
+    args = [("U", model.U), ("p", model.p)]
+    if isturbulent(model):
+        t = model.turbulence
+        args += [("k", t.k), ("omega", t.omega), ("nut", t.nut)]
+    write_vtk(name, model.mesh, *args)
 
 
 class Server:

@@ -20,6 +20,10 @@ ARRAY_FIELDS = (
 )
 
 
+# optional node data (mesh.nodes, mesh.cell_nodes), used by the VTK writer
+NODE_FIELDS = (("node_coords", np.float64), ("cell_nodes_ptr", np.int64), ("cell_nodes", np.int64))
+
+
 class Mesh2:
     """Flattened mesh.  ``boundaries`` lists patch names in file order;
     ``boundary_index(name)`` is 1-based like the reference."""
@@ -32,6 +36,9 @@ class Mesh2:
         self.patch_names = list(patch_names)
         for name, dt in ARRAY_FIELDS:
             setattr(self, name, np.ascontiguousarray(arrays[name], dtype=dt))
+        for name, dt in NODE_FIELDS:
+            setattr(self, name, np.ascontiguousarray(arrays.get(name, np.zeros(0)), dtype=dt))
+        self.nnodes = len(self.node_coords) // 3
         self._desc = None
 
     # --- reference helpers (src/Mesh/Mesh_1_functions.jl)
@@ -65,6 +72,11 @@ class Mesh2:
             ptype = _abi.P_d if dt == np.float64 else _abi.P_i64
             setattr(d, name, arr.ctypes.data_as(ptype))
         d.npatches = len(self.patch_names)
+        if self.nnodes > 0:
+            d.nnodes = self.nnodes
+            d.node_coords = self.node_coords.ctypes.data_as(_abi.P_d)
+            d.cell_nodes_ptr = self.cell_nodes_ptr.ctypes.data_as(_abi.P_i64)
+            d.cell_nodes = self.cell_nodes.ctypes.data_as(_abi.P_i64)
         self._desc = d
         return d
 
@@ -89,6 +101,11 @@ class Mesh2:
         for name, dt in ARRAY_FIELDS:
             n = shapes[name]
             arrays[name] = np.ctypeslib.as_array(getattr(d, name), shape=(n,)).copy() if n else np.zeros(0, dt)
+        if d.nnodes > 0 and d.cell_nodes_ptr:
+            cnp = np.ctypeslib.as_array(d.cell_nodes_ptr, shape=(nc + 1,)).copy()
+            arrays["node_coords"] = np.ctypeslib.as_array(d.node_coords, shape=(3 * d.nnodes,)).copy()
+            arrays["cell_nodes_ptr"] = cnp
+            arrays["cell_nodes"] = np.ctypeslib.as_array(d.cell_nodes, shape=(int(cnp[-1] - 1),)).copy()
         return cls(nc, nf, d.nbfaces, d.dim, patch_names, **arrays)
 
     @classmethod
@@ -98,4 +115,4 @@ class Mesh2:
 
     def copy(self):
         return Mesh2(self.ncells, self.nfaces, self.nbfaces, self.dim, self.patch_names,
-                     **{k: getattr(self, k).copy() for k, _ in ARRAY_FIELDS})
+                     **{k: getattr(self, k).copy() for k, _ in ARRAY_FIELDS + NODE_FIELDS})
