@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--serve-maxit", type=int, default=3000, help="per-case SIMPLE iteration cap")
     ap.add_argument("--slots", type=int, default=40, help="concurrent serving cases")
     ap.add_argument("--serve-check", type=int, default=4, help="cases re-run alone for the parity check")
+    ap.add_argument("--precision-report", type=int, default=0, metavar="ITERS",
+                    help="run ITERS SIMPLE iterations in FP64 and in mixed precision and report the "
+                         "relative L2 difference of every field and both timings (one JSON line)")
     ap.add_argument("--renumber", default="color", choices=["color", "rcm", "none"])
     ap.add_argument("--size", type=int, default=None,
                     help="bfs: cells per step height (27); cavity: cells per side (40); cavity3d: cells per side (128)")
@@ -304,9 +307,43 @@ def serve_main(a):
     print(json.dumps(line))
 
 
+# -------------------------------------------------------- precision report
+def precision_report(a):
+    """FP64 and mixed precision from the same initial fields, ITERS iterations
+    each; relative L2 of the mixed fields against the FP64 ones."""
+    import xcal as X
+    from xcal import _abi, cases
+    mesh, model, config, pref, desc = build_case(a.config, a.size)
+    its = a.precision_report
+    out = {}
+    for name, prec in (("fp64", _abi.PREC_FP64), ("mixed", _abi.PREC_MIXED)):
+        case, keep = X.make_case(model, config, pref, prec)
+        s = X.Solver(mesh, renumber=_abi.RENUMBER_COLOR)
+        s.setup(case)
+        U0, p0 = cases.fields(model)
+        for f, v in ((_abi.FIELD_UX, U0[0]), (_abi.FIELD_UY, U0[1]), (_abi.FIELD_UZ, U0[2]), (_abi.FIELD_P, p0)):
+            s.set_field(f, v)
+        r = s.run(its, want_krylov=True)
+        fields = {k: s.get_field(f) for k, f in (("Ux", _abi.FIELD_UX), ("Uy", _abi.FIELD_UY), ("Uz", _abi.FIELD_UZ),
+                                                  ("p", _abi.FIELD_P))}
+        out[name] = dict(ms=s.last_ms(), done=r["done"], fields=fields,
+                         R_last=[float(r[k][r["done"] - 1]) for k in ("R_ux", "R_uy", "R_uz", "R_p")],
+                         kry=r["krylov"][: r["done"]].mean(axis=0).tolist())
+        s.close()
+    rel = {k: float(np.linalg.norm(out["mixed"]["fields"][k] - out["fp64"]["fields"][k]) /
+                    max(np.linalg.norm(out["fp64"]["fields"][k]), 1e-300)) for k in ("Ux", "Uy", "Uz", "p")}
+    print(json.dumps({"metric": "mixed vs fp64 relative L2", "config": {"workload": desc, "cells": mesh.ncells,
+                      "iterations": its}, "rel_l2": rel,
+                      "fp64": {k: v for k, v in out["fp64"].items() if k != "fields"},
+                      "mixed": {k: v for k, v in out["mixed"].items() if k != "fields"},
+                      "speedup": out["fp64"]["ms"] / out["mixed"]["ms"]}))
+
+
 # -------------------------------------------------------------------- main
 def main():
     a = parse()
+    if a.precision_report:
+        return precision_report(a)
     if a.config == "serve":
         if a.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop "

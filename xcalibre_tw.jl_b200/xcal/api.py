@@ -269,10 +269,10 @@ def _solver(s, name):
     code = s["solver"].code
     pcode = s["preconditioner"].code
     if code is None:
-        raise _abi.XcalError(f"{name}: solver {s['solver'].__name__} is not available (CG, BiCGSTAB)")
+        raise _abi.XcalError(f"{name}: solver {s['solver'].__name__} is not available (CG, BiCGSTAB, GMRES)")
     if pcode is None:
         raise _abi.XcalError(f"{name}: preconditioner {s['preconditioner'].__name__} is not "
-                             "available (DILU, Jacobi, NormDiagonal)")
+                             "available (DILU, ILU0, Jacobi, NormDiagonal)")
     return _abi.SolverCfg(code, pcode, s["itmax"], 0, s["convergence"], s["relax"], s["atol"], s["rtol"])
 
 
