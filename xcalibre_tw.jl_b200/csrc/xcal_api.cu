@@ -63,8 +63,14 @@ struct xcal_ctx_s {
   double conv = 1e-7;          // SIMPLE stop tolerance
   int run_cap = 0;
   double last_ms = 0.0;
-  double *pin = nullptr;       // pinned staging [n*3]
+  double *pin = nullptr;       // pinned staging, one region of n values per field
   size_t pin_n = 0;
+  cudaEvent_t pin_ev[7] = {};  // last copy out of each pinned field region
+  bool pin_busy[7] = {};
+  int *d_perm = nullptr;       // caller cell -> device cell (device copy, int32)
+  double *d_stage = nullptr;   // device staging, one region of n values per field
+  void *rpin = nullptr;        // pinned run-result staging (barrier word, count, R, Krylov counts)
+  size_t rpin_n = 0;
   std::vector<BcEntry> tabU, tabP;
   std::vector<xcal_bc> bcU_host;   // the case's U conditions (post-processing)
 };
@@ -198,6 +204,11 @@ int xcal_ctx_create(int device, uint32_t flags, xcal_ctx *out) {
     return XCAL_ERR_CUDA;
   }
   c->mbuf.stream = c->cbuf.stream = c->rbuf.stream = c->stream;
+  for (auto &e : c->pin_ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      delete c;
+      return XCAL_ERR_CUDA;
+    }
   // Keep freed stream-ordered memory in the device's pool: with the default
   // release threshold (0) every synchronisation would hand it back and the
   // next set-up would map fresh memory again.
@@ -218,6 +229,9 @@ int xcal_ctx_destroy(xcal_ctx c) {
   c->cbuf.release();
   c->mbuf.release();
   if (c->pin) cudaFreeHost(c->pin);
+  if (c->rpin) cudaFreeHost(c->rpin);
+  for (auto &e : c->pin_ev)
+    if (e) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -383,6 +397,12 @@ int xcal_mesh_upload(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
   TRY(upload_c(c, B, ecol, P.e_col)); TRY(upload_c(c, B, etpos, P.e_tpos)); TRY(upload_c(c, B, edpos, P.dpos));
   for (Mat *A : {&h.AU, &h.AP}) { A->col = ecol; A->tpos = etpos; A->dpos = edpos; A->W = P.W; A->np = P.np; }
   choose_launch(c, P.n, h);
+  {
+    std::vector<int> p32(c->perm.begin(), c->perm.end());
+    const int *dp = nullptr;
+    TRY(upload_c(c, B, dp, p32));
+    c->d_perm = const_cast<int *>(dp);
+  }
   c->have_mesh = true;
   return XCAL_OK;
 }
@@ -612,12 +632,16 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   CUDA_TRY(c, zero_dev(c, h.AP.val, sizeof(double) * nnz));
   CUDA_TRY(c, zero_dev(c, h.bU, sizeof(double) * n * NS));
   CUDA_TRY(c, zero_dev(c, h.bP, sizeof(double) * n));
-  if (!c->pin || c->pin_n < (size_t)n * 3) {
+  if (!c->pin || c->pin_n < (size_t)n * 7) {
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     if (c->pin) cudaFreeHost(c->pin);
     c->pin = nullptr;
-    CUDA_TRY(c, cudaMallocHost(&c->pin, sizeof(double) * n * 3));
-    c->pin_n = (size_t)n * 3;
+    CUDA_TRY(c, cudaMallocHost(&c->pin, sizeof(double) * n * 7));
+    c->pin_n = (size_t)n * 7;
   }
+  for (bool &b : c->pin_busy) b = false;
+  c->d_stage = B.alloc<double>((size_t)n * 7);
+  if (!c->d_stage) return fail(c, XCAL_ERR_OOM, "device allocation failed");
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->have_case = true;
   return XCAL_OK;
@@ -643,6 +667,12 @@ static int field_target(xcal_ctx c, int32_t field, double *&base, int &stride, i
   }
 }
 
+// Field transfer.  A context's fields live in device numbering, components
+// interleaved.  Ordinary contexts copy the caller's array contiguously
+// (pinned staging, one region per field) and scatter/gather with a small
+// kernel applying the permutation; xcal_field_set returns without waiting
+// for the copy.  Cluster-mode contexts (the serving loop) keep to copy
+// engines only: a kernel could wait for SMs held by other contexts' runs.
 int xcal_field_set(xcal_ctx c, int32_t field, const double *host, int64_t n) {
   if (!c || !host) return XCAL_ERR_ARG;
   if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_field_set before xcal_case_setup");
@@ -650,12 +680,23 @@ int xcal_field_set(xcal_ctx c, int32_t field, const double *host, int64_t n) {
   double *base; int stride, off;
   TRY(field_target(c, field, base, stride, off));
   CUDA_TRY(c, cudaSetDevice(c->device));
-  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  double *st = c->pin;
-  for (int64_t i = 0; i < n; ++i) st[c->perm[i]] = host[i];
-  CUDA_TRY(c, cudaMemcpy2DAsync(base + off, sizeof(double) * stride, st, sizeof(double), sizeof(double), n,
-                                cudaMemcpyHostToDevice, c->stream));
-  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  double *hs = c->pin + (size_t)field * n;
+  if (c->pin_busy[field]) {
+    CUDA_TRY(c, cudaEventSynchronize(c->pin_ev[field]));
+    c->pin_busy[field] = false;
+  }
+  if (c->flags & XCAL_FLAG_CLUSTER) {
+    for (int64_t i = 0; i < n; ++i) hs[c->perm[i]] = host[i];
+    CUDA_TRY(c, cudaMemcpy2DAsync(base + off, sizeof(double) * stride, hs, sizeof(double), sizeof(double), n,
+                                  cudaMemcpyHostToDevice, c->stream));
+  } else {
+    std::memcpy(hs, host, sizeof(double) * n);
+    double *ds = c->d_stage + (size_t)field * n;
+    CUDA_TRY(c, cudaMemcpyAsync(ds, hs, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, launch_field_scatter((int)n, ds, c->d_perm, base + off, stride, c->stream));
+  }
+  CUDA_TRY(c, cudaEventRecord(c->pin_ev[field], c->stream));
+  c->pin_busy[field] = true;
   return XCAL_OK;
 }
 
@@ -666,11 +707,20 @@ int xcal_field_get(xcal_ctx c, int32_t field, double *host, int64_t n) {
   double *base; int stride, off;
   TRY(field_target(c, field, base, stride, off));
   CUDA_TRY(c, cudaSetDevice(c->device));
-  double *st = c->pin;
-  CUDA_TRY(c, cudaMemcpy2DAsync(st, sizeof(double), base + off, sizeof(double) * stride, sizeof(double), n,
-                                cudaMemcpyDeviceToHost, c->stream));
-  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  for (int64_t i = 0; i < n; ++i) host[i] = st[c->perm[i]];
+  double *hs = c->pin + (size_t)field * n;
+  if (c->flags & XCAL_FLAG_CLUSTER) {
+    CUDA_TRY(c, cudaMemcpy2DAsync(hs, sizeof(double), base + off, sizeof(double) * stride, sizeof(double), n,
+                                  cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (int64_t i = 0; i < n; ++i) host[i] = hs[c->perm[i]];
+  } else {
+    double *ds = c->d_stage + (size_t)field * n;
+    CUDA_TRY(c, launch_field_gather((int)n, base + off, c->d_perm, ds, stride, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(hs, ds, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    std::memcpy(host, hs, sizeof(double) * n);
+  }
+  c->pin_busy[field] = false;
   return XCAL_OK;
 }
 
@@ -700,27 +750,39 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
   if (iters > 0) CUDA_TRY(c, launch_program(c->ns, h.prec == XCAL_PREC_MIXED, c->mode, c->nblocks, &h, prog, iters, c->stream));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+  // results: one pinned block, one synchronisation
+  const size_t nR = (size_t)std::max(iters, 1) * 4, nK = (size_t)std::max(iters, 1) * 5;
+  const size_t need = sizeof(Bar) + 16 + sizeof(double) * nR + sizeof(int) * nK;
+  if (!c->rpin || c->rpin_n < need) {
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (c->rpin) cudaFreeHost(c->rpin);
+    c->rpin = nullptr;
+    CUDA_TRY(c, cudaMallocHost(&c->rpin, need));
+    c->rpin_n = need;
+  }
+  Bar *hb = (Bar *)c->rpin;
+  int *hdn = (int *)((char *)c->rpin + sizeof(Bar));
+  double *R = (double *)((char *)c->rpin + sizeof(Bar) + 16);
+  int *K = (int *)(R + nR);
+  CUDA_TRY(c, cudaMemcpyAsync(hb, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(hdn, h.done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (iters > 0) {
+    CUDA_TRY(c, cudaMemcpyAsync(R, h.R, sizeof(double) * iters * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (kry) CUDA_TRY(c, cudaMemcpyAsync(K, h.kry, sizeof(int) * iters * 5, cudaMemcpyDeviceToHost, c->stream));
+  }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
-  Bar bar;
-  int dn = 0;
-  CUDA_TRY(c, copy_sync(c, &bar, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost));
-  CUDA_TRY(c, copy_sync(c, &dn, h.done, sizeof(int), cudaMemcpyDeviceToHost));
-  std::vector<double> R((size_t)std::max(iters, 1) * 4);
-  std::vector<int> K((size_t)std::max(iters, 1) * 5);
-  if (iters > 0) {
-    CUDA_TRY(c, copy_sync(c, R.data(), h.R, sizeof(double) * iters * 4, cudaMemcpyDeviceToHost));
-    CUDA_TRY(c, copy_sync(c, K.data(), h.kry, sizeof(int) * iters * 5, cudaMemcpyDeviceToHost));
-  }
+  const Bar bar = *hb;
+  const int dn = *hdn;
   for (int i = 0; i < iters; ++i) {
     if (Rux) Rux[i] = R[4 * i];
     if (Ruy) Ruy[i] = R[4 * i + 1];
     if (Ruz) Ruz[i] = R[4 * i + 2];
     if (Rp) Rp[i] = R[4 * i + 3];
   }
-  if (kry) std::copy(K.begin(), K.begin() + (size_t)iters * 5, kry);
+  if (kry) std::copy(K, K + (size_t)iters * 5, kry);
   if (done) *done = dn;
   if (bar.err) return fail(c, XCAL_ERR_TIMEOUT, "device barrier timed out");
   if (bar.nonfinite)

@@ -5,6 +5,7 @@
 //   and the canonical reduction of xcal_device.cuh.
 // xcal_residual_noalloc: the same kernels for callers that must not allocate
 //   device memory, with the per-tile partial sums in a fixed file-scope array.
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -88,5 +89,30 @@ cudaError_t noalloc_scratch(int device, double **out) {
 }
 
 int noalloc_max_rows() { return XCAL_NOALLOC_MAX_TILES * TILE; }
+
+
+__global__ void __launch_bounds__(TPB) field_scatter_kernel(int n, const double *__restrict__ src,
+                                                            const int *__restrict__ perm, double *dst, int stride) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) dst[(size_t)perm[i] * stride] = src[i];
+}
+
+__global__ void __launch_bounds__(TPB) field_gather_kernel(int n, const double *src, const int *__restrict__ perm,
+                                                           double *__restrict__ dst, int stride) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) dst[i] = src[(size_t)perm[i] * stride];
+}
+
+static int field_grid(int n) { return std::max(1, std::min((n + TPB - 1) / TPB, 148 * 8)); }
+
+cudaError_t launch_field_scatter(int n, const double *src, const int *perm, double *dst, int stride,
+                                 cudaStream_t stream) {
+  field_scatter_kernel<<<field_grid(n), TPB, 0, stream>>>(n, src, perm, dst, stride);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_field_gather(int n, const double *src, const int *perm, double *dst, int stride,
+                                cudaStream_t stream) {
+  field_gather_kernel<<<field_grid(n), TPB, 0, stream>>>(n, src, perm, dst, stride);
+  return cudaGetLastError();
+}
 
 }  // namespace xcal
