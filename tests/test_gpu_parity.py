@@ -101,6 +101,23 @@ def test_cg_fused_and_split_phases(fuse, monkeypatch):
     assert_parity(dev, orc, nU=3)
 
 
+@pytest.mark.parametrize("occ", ["2", "4"])
+def test_occupancy_builds_match_oracle(occ, monkeypatch):
+    """The 2-CTA/SM and 4-CTA/SM builds of the persistent program (forced
+    with XCAL_OCC, grid barrier) compute the same values: bitwise equal to the
+    oracle on the 2D BFS and the 3D cavity, FP64."""
+    monkeypatch.setenv("XCAL_OCC", occ)
+    monkeypatch.setenv("XCAL_SYNC", "grid")
+    mesh, model, config, pref = cases.bfs(6, iterations=30)
+    dev = run_device(mesh, model, config, pref, 30, _abi.RENUMBER_COLOR)
+    orc = run_oracle(dev["dev_mesh"], model, config, pref, 30, dev["perm"])
+    assert_parity(dev, orc)
+    mesh, model, config, pref = cases.cavity3d(12, iterations=10)
+    dev = run_device(mesh, model, config, pref, 10, _abi.RENUMBER_COLOR)
+    orc = run_oracle(dev["dev_mesh"], model, config, pref, 10, dev["perm"])
+    assert_parity(dev, orc, nU=3)
+
+
 def _snapshot_matrix(n=24, iters=5):
     mesh, model, config, pref = cases.cavity2d(n, iterations=iters)
     om = O.from_mesh2(mesh)

@@ -19,10 +19,13 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "--fmad=false", "-lineinfo",
          "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "--expt-relaxed-constexpr", "-diag-suppress=177"]
-INSTANCES = {"d1": (1, "double"), "d2": (2, "double"), "d3": (3, "double"), "f2": (2, "float"),
-             "f3": (3, "float")}
-UNITS = [("xcal_kernel.cu", tag, ["-DXCAL_INST=" + tag, f"-DXCAL_NS={ns}", f"-DXCAL_T={t}"])
-         for tag, (ns, t) in INSTANCES.items()]
+# instantiation tag -> (components, Krylov value type, resident CTAs per SM the
+# register budget is sized for); the "o" builds trade spills for occupancy
+INSTANCES = {"d1": (1, "double", 2), "d2": (2, "double", 2), "d3": (3, "double", 2), "f2": (2, "float", 2),
+             "f3": (3, "float", 2), "d2o": (2, "double", 4), "d3o": (3, "double", 4), "f2o": (2, "float", 4),
+             "f3o": (3, "float", 4)}
+UNITS = [("xcal_kernel.cu", tag, ["-DXCAL_INST=" + tag, f"-DXCAL_NS={ns}", f"-DXCAL_T={t}", f"-DXCAL_MB={mb}"])
+         for tag, (ns, t, mb) in INSTANCES.items()]
 UNITS += [("xcal_launch.cu", None, []), ("xcal_ops.cu", None, []), ("xcal_api.cu", None, []),
           ("host_mesh.cpp", None, []), ("xcal_serve.cpp", None, [])]
 

@@ -58,6 +58,7 @@ struct xcal_ctx_s {
   Prep prep;
   int ns = 2;
   int mode = SYNC_GRID, nblocks = 1;
+  int occ = 0;                 // program build: 0 = 2 CTAs/SM, 1 = 4 CTAs/SM (xcal_kernel.h)
   DevBuf mbuf, cbuf, rbuf;     // mesh, case, run buffers
   KParams hp;
   double conv = 1e-7;          // SIMPLE stop tolerance
@@ -145,12 +146,31 @@ static void choose_launch(xcal_ctx c, int n, KParams &h) {
   h.cg_fuse = choose_cg_fuse((n + TILE - 1) / TILE, c->nblocks);
 }
 
+// Build of the persistent program for a grid launch: the 4-CTA/SM build once
+// the mesh has more tiles than the 2-CTA/SM grid has CTAs (the phases are
+// then memory-latency rather than barrier bound).  Measured on B200, ms per
+// SIMPLE iteration (2-CTA / 4-CTA build): BFS 47k cells, 186 tiles 1.50 / 1.73;
+// cavity 32^3, 128 tiles 0.86 / 0.96; 48^3, 432 tiles 1.71 / 1.62; 64^3
+// 3.56 / 2.93; 96^3 15.4 / 11.8; 128^3 39.6 / 27.7.  XCAL_OCC=2 or 4 forces
+// one.  Both builds compute the same values.
+constexpr int OCC_TILES_PER_CTA = 1;
+static int choose_occ(xcal_ctx c, int ntiles) {
+  const char *o = getenv("XCAL_OCC");
+  if (o) return atoi(o) == 4 ? 1 : 0;
+  if (c->ns < 2) return 0;
+  const int maxco2 = max_coresident_blocks(c->ns, 0, c->device);
+  return ntiles > OCC_TILES_PER_CTA * std::max(maxco2, 1) ? 1 : 0;
+}
+
 static void choose_launch_mode(xcal_ctx c, int n) {
   int ntiles = (n + TILE - 1) / TILE;
   const char *m = getenv("XCAL_SYNC");
   const char *nbv = getenv("XCAL_NBLOCKS");
   int ns = c->ns;
-  int maxco = max_coresident_blocks(ns, c->device);
+  c->occ = 0;
+  if (!(c->flags & XCAL_FLAG_CLUSTER) && !(m && (!strcmp(m, "block") || !strcmp(m, "cluster"))))
+    c->occ = choose_occ(c, ntiles);
+  int maxco = max_coresident_blocks(ns, c->occ, c->device);
   if (m && !strcmp(m, "block")) { c->mode = SYNC_BLOCK; c->nblocks = 1; return; }
   if ((c->flags & XCAL_FLAG_CLUSTER) && !m) {   // one hardware cluster: safe beside other kernels
     c->mode = SYNC_CLUSTER;
@@ -174,6 +194,7 @@ static void choose_launch_mode(xcal_ctx c, int n) {
   if (ntiles <= mc) {
     c->mode = SYNC_CLUSTER;
     c->nblocks = std::max(1, ntiles);
+    c->occ = 0;
   } else {
     c->mode = SYNC_GRID;
     c->nblocks = std::max(1, std::min(maxco, ntiles));
@@ -748,7 +769,9 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   h.conv = c->conv;
   h.abort_nan = (c->flags & XCAL_FLAG_ABORT_ON_NAN) ? 1 : 0;
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-  if (iters > 0) CUDA_TRY(c, launch_program(c->ns, h.prec == XCAL_PREC_MIXED, c->mode, c->nblocks, &h, prog, iters, c->stream));
+  if (iters > 0)
+    CUDA_TRY(c, launch_program(c->ns, h.prec == XCAL_PREC_MIXED, c->occ, c->mode, c->nblocks, &h, prog, iters,
+                               c->stream));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   // results: one pinned block, one synchronisation
   const size_t nR = (size_t)std::max(iters, 1) * 4, nK = (size_t)std::max(iters, 1) * 5;
@@ -924,11 +947,11 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   h.solve_solver = solver; h.solve_itmax = itmax; h.solve_atol = atol; h.solve_rtol = rtol;
   int mode, nb;
   {
-    int saved_ns = c->ns, saved_mode = c->mode, saved_nb = c->nblocks;
+    int saved_ns = c->ns, saved_mode = c->mode, saved_nb = c->nblocks, saved_occ = c->occ;
     c->ns = 1;
     choose_launch(c, n, h);
     mode = c->mode; nb = c->nblocks;
-    c->ns = saved_ns; c->mode = saved_mode; c->nblocks = saved_nb;
+    c->ns = saved_ns; c->mode = saved_mode; c->nblocks = saved_nb; c->occ = saved_occ;
   }
   h.mode = mode;
   if (solver == XCAL_SOLVER_GMRES) {
@@ -938,7 +961,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
     if (!ok) return fail(c, XCAL_ERR_OOM, "device allocation failed");
   }
   CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
-  CUDA_TRY(c, launch_program(1, 0, mode, nb, &h, PROG_SOLVE, 1, c->stream));
+  CUDA_TRY(c, launch_program(1, 0, 0, mode, nb, &h, PROG_SOLVE, 1, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   Bar bar;
   double so[2];

@@ -1637,9 +1637,13 @@ __device__ void solve_program(Ctx &C) {
 
 // KParams is passed by value: the fields live in the kernel's constant
 // parameter bank instead of occupying registers.  T is the scalar type of
-// the Krylov iterations (double: FP64 path; float: mixed path).
-template <int NS, typename T>
-__global__ void __launch_bounds__(TPB, 2) xcal_program_kernel(const __grid_constant__ KParams prm, int prog, int iters) {
+// the Krylov iterations (double: FP64 path; float: mixed path).  MB is the
+// number of resident CTAs per SM the register budget is sized for: 2 (128
+// registers, few spills) suits meshes with about one tile per CTA, where a
+// phase is barrier-latency bound; 4 (64 registers, more spills, twice the
+// warps in flight) suits large meshes, where a phase is memory-latency bound.
+template <int NS, typename T, int MB>
+__global__ void __launch_bounds__(TPB, MB) xcal_program_kernel(const __grid_constant__ KParams prm, int prog, int iters) {
   __shared__ double sm[8 * MAXK];
   __shared__ double sm_out[MAXK];
   __shared__ double ws[MAXTL * MAXK * 8];
@@ -1666,8 +1670,13 @@ __global__ void __launch_bounds__(TPB, 2) xcal_program_kernel(const __grid_const
 #if defined(XCAL_INST)
 #define XCAL_CAT2(a, b) a##b
 #define XCAL_CAT(a, b) XCAL_CAT2(a, b)
-template __global__ void xcal_program_kernel<XCAL_NS, XCAL_T>(const __grid_constant__ KParams, int, int);
-const void *XCAL_CAT(program_kernel_, XCAL_INST)() { return (const void *)xcal_program_kernel<XCAL_NS, XCAL_T>; }
+#ifndef XCAL_MB
+#define XCAL_MB 2
+#endif
+template __global__ void xcal_program_kernel<XCAL_NS, XCAL_T, XCAL_MB>(const __grid_constant__ KParams, int, int);
+const void *XCAL_CAT(program_kernel_, XCAL_INST)() {
+  return (const void *)xcal_program_kernel<XCAL_NS, XCAL_T, XCAL_MB>;
+}
 #endif
 
 }  // namespace xcal

@@ -5,9 +5,11 @@
 #include "xcal_device.cuh"
 
 namespace xcal {
-cudaError_t launch_program(int ns, int mixed, int mode, int nblocks, const KParams *hparams, int prog, int iters,
-                           cudaStream_t stream);
-int max_coresident_blocks(int ns, int device);
+// occ selects the build: 0 = two resident CTAs per SM (128 registers),
+// 1 = four (64 registers); the NS = 1 standalone-solve program has only the first.
+cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, const KParams *hparams, int prog,
+                           int iters, cudaStream_t stream);
+int max_coresident_blocks(int ns, int occ, int device);
 int max_cluster_blocks(int ns);
-const void *program_kernel_ptr(int ns, int mixed);
+const void *program_kernel_ptr(int ns, int mixed, int occ);
 }  // namespace xcal

@@ -13,16 +13,24 @@ const void *program_kernel_d2();
 const void *program_kernel_d3();
 const void *program_kernel_f2();
 const void *program_kernel_f3();
+const void *program_kernel_d2o();
+const void *program_kernel_d3o();
+const void *program_kernel_f2o();
+const void *program_kernel_f3o();
 
-const void *program_kernel_ptr(int ns, int mixed) {
+const void *program_kernel_ptr(int ns, int mixed, int occ) {
   if (ns == 1) return program_kernel_d1();
-  if (ns == 2) return mixed ? program_kernel_f2() : program_kernel_d2();
+  if (ns == 2) {
+    if (occ) return mixed ? program_kernel_f2o() : program_kernel_d2o();
+    return mixed ? program_kernel_f2() : program_kernel_d2();
+  }
+  if (occ) return mixed ? program_kernel_f3o() : program_kernel_d3o();
   return mixed ? program_kernel_f3() : program_kernel_d3();
 }
 
-cudaError_t launch_program(int ns, int mixed, int mode, int nblocks, const KParams *hparams, int prog, int iters,
-                           cudaStream_t stream) {
-  const void *fn = program_kernel_ptr(ns, mixed);
+cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, const KParams *hparams, int prog,
+                           int iters, cudaStream_t stream) {
+  const void *fn = program_kernel_ptr(ns, mixed, occ);
   void *args[3];
   args[0] = (void *)hparams;
   args[1] = (void *)&prog;
@@ -48,11 +56,11 @@ cudaError_t launch_program(int ns, int mixed, int mode, int nblocks, const KPara
   return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(TPB), args, 0, stream);
 }
 
-int max_coresident_blocks(int ns, int device) {
+int max_coresident_blocks(int ns, int occ, int device) {
   int per_sm = 0, sms = 0, per_sm32 = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, program_kernel_ptr(ns, 0), TPB, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, program_kernel_ptr(ns, 0, occ), TPB, 0);
   if (ns >= 2) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, program_kernel_ptr(ns, 1), TPB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, program_kernel_ptr(ns, 1, occ), TPB, 0);
     per_sm = std::min(per_sm, per_sm32);
   }
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -60,7 +68,7 @@ int max_coresident_blocks(int ns, int device) {
 }
 
 int max_cluster_blocks(int ns) {
-  const void *fn = program_kernel_ptr(ns, 0);
+  const void *fn = program_kernel_ptr(ns, 0, 0);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 8;
   for (int c = 16; c >= 1; c >>= 1) {
     cudaLaunchConfig_t cfg = {};
