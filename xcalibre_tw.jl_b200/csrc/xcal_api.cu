@@ -147,19 +147,23 @@ static void choose_launch(xcal_ctx c, int n, KParams &h) {
 }
 
 // Build of the persistent program for a grid launch: the 4-CTA/SM build once
-// the mesh has more tiles than the 2-CTA/SM grid has CTAs (the phases are
-// then memory-latency rather than barrier bound).  Measured on B200, ms per
-// SIMPLE iteration (2-CTA / 4-CTA build): BFS 47k cells, 186 tiles 1.50 / 1.73;
-// cavity 32^3, 128 tiles 0.86 / 0.96; 48^3, 432 tiles 1.71 / 1.62; 64^3
-// 3.56 / 2.93; 96^3 15.4 / 11.8; 128^3 39.6 / 27.7.  XCAL_OCC=2 or 4 forces
-// one.  Both builds compute the same values.
-constexpr int OCC_TILES_PER_CTA = 1;
+// the mesh has more tiles per CTA of the 2-CTA/SM grid than a threshold (the
+// phases are then memory-latency rather than barrier bound).  Measured on
+// B200, ms per SIMPLE iteration (2-CTA / 4-CTA build), 296-CTA grid:
+//   3D: cavity 32^3 (128 tiles) 0.86 / 0.96; 48^3 (432) 1.71 / 1.62;
+//       64^3 (1024) 3.56 / 2.93; 96^3 (3456) 15.4 / 11.8; 128^3 (8192) 39.6 / 27.7
+//   2D: BFS 47k (186) 1.50 / 1.73; BFS 104k (407) 1.97 / 1.96; flat plate k-omega
+//       150k (586) 2.68 / 2.77; cavity 400^2 (625) 2.53 / 2.71; BFS 190k (741)
+//       2.80 / 2.73; BFS 416k (1625) 4.62 / 3.95; cavity 800^2 (2500) 6.86 / 6.42
+// so the threshold is 1 tile per CTA in 3D and 3 in 2D.  XCAL_OCC=2 or 4
+// forces one.  Both builds compute the same values.
 static int choose_occ(xcal_ctx c, int ntiles) {
   const char *o = getenv("XCAL_OCC");
   if (o) return atoi(o) == 4 ? 1 : 0;
   if (c->ns < 2) return 0;
   const int maxco2 = max_coresident_blocks(c->ns, 0, c->device);
-  return ntiles > OCC_TILES_PER_CTA * std::max(maxco2, 1) ? 1 : 0;
+  const int per_cta = (c->ns == 3) ? 1 : 3;
+  return ntiles > per_cta * std::max(maxco2, 1) ? 1 : 0;
 }
 
 static void choose_launch_mode(xcal_ctx c, int n) {
