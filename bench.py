@@ -339,6 +339,37 @@ def precision_report(a):
                       "speedup": out["fp64"]["ms"] / out["mixed"]["ms"]}))
 
 
+# ------------------------------------------------------------------- ranks
+def init_ranks(world, local, backend="nccl", timeout_s=120):
+    """One process per GPU: set the device and join the process group (None
+    for a single rank).  The group carries only the timing barrier and the
+    max-over-ranks reduction, never case data."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, init_method="env://", timeout=datetime.timedelta(seconds=timeout_s))
+    return dist
+
+
+def max_over_ranks(x, dist, device):
+    """The largest per-rank value (the slowest replica sets the job's time)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, units_per_rank, seconds):
+    """Whole-job rate: every rank processed units_per_rank in at most `seconds`."""
+    return world * units_per_rank / seconds
+
+
 # -------------------------------------------------------------------- main
 def main():
     a = parse()
@@ -375,12 +406,7 @@ def main():
         return
 
     import torch
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        dist = dist_mod
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    dist = init_ranks(world, local)
     import xcal as X
     from xcal import _abi, cases
 
@@ -427,12 +453,8 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    total_ms = float(sum(ms))
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * N * a.steps / (total_ms / 1000.0)
+    total_ms = max_over_ranks(float(sum(ms)), dist, dev)
+    value = job_throughput(world, N * a.steps, total_ms / 1000.0)
     kry = np.array(kry)
     # roofline of the (single) device program kernel
     ns = 3 if mesh.dim == 3 else 2
@@ -454,11 +476,7 @@ def main():
         out = s.run(1, want_krylov=False)
         Uh[0] = s.get_field(_abi.FIELD_UX); Uh[1] = s.get_field(_abi.FIELD_UY); ph = s.get_field(_abi.FIELD_P)
         e2e_t += time.perf_counter() - t0
-    e2e_value = world * N * e2e_steps / e2e_t
-    if dist:
-        t = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = world * N * e2e_steps / float(t.item())
+    e2e_value = job_throughput(world, N * e2e_steps, max_over_ranks(e2e_t, dist, dev))
     h2d = 3 * N * 8
     d2h = 3 * N * 8 + 4 * 8 + 5 * 4
     s.close()
