@@ -56,20 +56,37 @@ cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, co
   return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(TPB), args, 0, stream);
 }
 
+// Occupancy probes: a failed query counts as zero and its error is consumed
+// here, so that it is not reported later by an unrelated call that reads the
+// runtime's last error.
 int max_coresident_blocks(int ns, int occ, int device) {
   int per_sm = 0, sms = 0, per_sm32 = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, program_kernel_ptr(ns, 0, occ), TPB, 0);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, program_kernel_ptr(ns, 0, occ), TPB, 0) !=
+      cudaSuccess) {
+    (void)cudaGetLastError();
+    per_sm = 0;
+  }
   if (ns >= 2) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, program_kernel_ptr(ns, 1, occ), TPB, 0);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, program_kernel_ptr(ns, 1, occ), TPB, 0) !=
+        cudaSuccess) {
+      (void)cudaGetLastError();
+      per_sm32 = 0;
+    }
     per_sm = std::min(per_sm, per_sm32);
   }
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    (void)cudaGetLastError();
+    sms = 0;
+  }
   return per_sm * sms;
 }
 
 int max_cluster_blocks(int ns) {
   const void *fn = program_kernel_ptr(ns, 0, 0);
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 8;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 8;
+  }
   for (int c = 16; c >= 1; c >>= 1) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(c);
@@ -82,7 +99,11 @@ int max_cluster_blocks(int ns) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) == cudaSuccess && nclusters >= 1) return c;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) != cudaSuccess) {
+      (void)cudaGetLastError();   // this cluster size is not possible: try the next smaller
+      continue;
+    }
+    if (nclusters >= 1) return c;
   }
   return 1;
 }

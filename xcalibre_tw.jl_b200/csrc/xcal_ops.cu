@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(TPB) residual_final_kernel(int n, const double
 cudaError_t launch_residual(int n, const int *rp, const int *col, const double *val, const double *x,
                             const double *b, double *part, double *out, cudaStream_t stream) {
   const int ntiles = (n + TILE - 1) / TILE;
+  (void)cudaGetLastError();   // report this launch's error, not an earlier call's
   residual_tiles_kernel<<<ntiles, TPB, 0, stream>>>(n, rp, col, val, x, b, part, ntiles);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -105,12 +106,14 @@ static int field_grid(int n) { return std::max(1, std::min((n + TPB - 1) / TPB, 
 
 cudaError_t launch_field_scatter(int n, const double *src, const int *perm, double *dst, int stride,
                                  cudaStream_t stream) {
+  (void)cudaGetLastError();   // report this launch's error, not an earlier call's
   field_scatter_kernel<<<field_grid(n), TPB, 0, stream>>>(n, src, perm, dst, stride);
   return cudaGetLastError();
 }
 
 cudaError_t launch_field_gather(int n, const double *src, const int *perm, double *dst, int stride,
                                 cudaStream_t stream) {
+  (void)cudaGetLastError();   // report this launch's error, not an earlier call's
   field_gather_kernel<<<field_grid(n), TPB, 0, stream>>>(n, src, perm, dst, stride);
   return cudaGetLastError();
 }
