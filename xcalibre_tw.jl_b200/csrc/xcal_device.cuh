@@ -233,11 +233,16 @@ __device__ __forceinline__ void block_tree(double (&s)[K], double *sm /* [8*K] *
   }
 }
 
-// Final sum of K partial arrays part[k*ntiles + t]; the result is broadcast
-// to every thread of the CTA.
+// Final sum of K partial arrays part[k*ntiles + t]; every thread of the CTA
+// obtains the result.  Same tree as block_tree: each thread evaluates the
+// 8-way stage itself from the staged warp sums, in the pairing of the
+// shuffle-down tree (4, 2, 1), so no broadcast and only two block barriers
+// are needed.  sm is free again once every thread has passed the next
+// barrier, which any later writer of sm executes before writing.
 template <int K>
 __device__ __forceinline__ void final_sum(const double *part, int ntiles, double *sm, double *sm_out,
                                           double (&out)[K]) {
+  (void)sm_out;
   double s[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
@@ -247,14 +252,25 @@ __device__ __forceinline__ void final_sum(const double *part, int ntiles, double
     for (int q = t + TPB; q < ntiles; q += TPB) a = a + pp[q];
     s[k] = a;
   }
-  block_tree<K>(s, sm);
-  if (threadIdx.x == 0)
 #pragma unroll
-    for (int k = 0; k < K; ++k) sm_out[k] = s[k];
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) s[k] = s[k] + __shfl_down_sync(0xffffffffu, s[k], off);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) sm[k * 8 + wid] = s[k];
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < K; ++k) out[k] = sm_out[k];
-  __syncthreads();
+  for (int k = 0; k < K; ++k) {
+    const double *w = sm + k * 8;
+    double a0 = w[0] + w[4], a1 = w[1] + w[5];
+    const double a2 = w[2] + w[6], a3 = w[3] + w[7];
+    a0 = a0 + a2;
+    a1 = a1 + a3;
+    out[k] = a0 + a1;
+  }
 }
 
 // ------------------------------------------------------------- sparse rows
