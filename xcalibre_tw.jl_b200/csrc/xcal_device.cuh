@@ -159,6 +159,17 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 
 __device__ __forceinline__ int ld_volatile_i32(const int *p) { return *(volatile const int *)p; }
 
+// Arrive: add with acquire-release semantics at GPU scope.  Release: the
+// CTA's writes, ordered before it by the preceding block barrier, become
+// visible with it.  Acquire: the last CTA to arrive (which does not poll)
+// reads the count through the chain of earlier arrivals and so sees their
+// writes.
+__device__ __forceinline__ unsigned long long atom_add_acqrel_u64(unsigned long long *p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+
 constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;   // 2 s
 
 // Barrier over all CTAs of the launch.  The grid form spins with a wall-clock
@@ -182,8 +193,7 @@ struct Sync {
     if (threadIdx.x == 0) {
       int good = 1;
       const unsigned long long target = epoch * (unsigned long long)nb;
-      __threadfence();
-      const unsigned long long v = atomicAdd(&bar->count, 1ull) + 1ull;
+      const unsigned long long v = atom_add_acqrel_u64(&bar->count, 1ull) + 1ull;
       if (v < target) {
         const unsigned long long t0 = globaltimer();
         unsigned spins = 0;
@@ -199,7 +209,8 @@ struct Sync {
           }
         }
       }
-      __threadfence();
+      // the acquire (poll, or the arrive of the last CTA) orders the CTA's
+      // later loads, through the block barrier below, after every arrive
       *ok = good;
     }
     __syncthreads();
