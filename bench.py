@@ -20,6 +20,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -133,7 +134,7 @@ def algorithmic_bytes(mesh, kry, ns, sk=8):
 class ClockSampler:
     def __init__(self, gpu_index):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"xcal_clocks_{os.getpid()}.csv")
         self.gpu = gpu_index
 
     def __enter__(self):
