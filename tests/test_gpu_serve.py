@@ -20,7 +20,7 @@ TOL = 1e-6
 MAXIT = 3000
 
 
-def _alone(c, precision):
+def _alone(c, precision, maxit=MAXIT):
     case, keep = X.make_case(c["model"], c["config"], c["pref"], precision)
     s = X.Solver(c["mesh"], renumber=_abi.RENUMBER_COLOR)
     try:
@@ -29,7 +29,7 @@ def _alone(c, precision):
         U, p = cases.fields(c["model"])
         for f, v in ((_abi.FIELD_UX, U[0]), (_abi.FIELD_UY, U[1]), (_abi.FIELD_UZ, U[2]), (_abi.FIELD_P, p)):
             s.set_field(f, v)
-        out = s.run(MAXIT, want_krylov=False)
+        out = s.run(maxit, want_krylov=False)
         out["U"] = np.stack([s.get_field(_abi.FIELD_UX), s.get_field(_abi.FIELD_UY), s.get_field(_abi.FIELD_UZ)])
         out["p"] = s.get_field(_abi.FIELD_P)
     finally:
@@ -101,3 +101,19 @@ def test_serve_stops_a_diverged_case():
     assert rb["status"] == -5 and rb["iterations"] == 1
     assert rg["status"] == 0 and rg["converged"] == 1
     assert st["failed"] == 1 and st["completed"] == 1
+
+
+def test_serve_large_case_matches_alone():
+    """A case with more tiles than three per CTA of its 16-CTA cluster runs on
+    the 4-CTA/SM build of the program inside the serving loop; its result
+    equals the case run alone (grid launch, 2-CTA/SM build) bit for bit."""
+    mesh, model, config, pref = cases.cavity2d(120, iterations=1)
+    c = dict(mesh=mesh, model=model, config=config, pref=pref)
+    srv = X.Server(slots=1, max_iterations=400, tolerance=TOL)
+    try:
+        r = srv.poll(srv.submit(model, config, pref, _abi.PREC_FP64), wait_ms=-1)
+    finally:
+        srv.close()
+    a = _alone(c, _abi.PREC_FP64, maxit=400)
+    assert r["status"] == 0 and r["iterations"] == a["done"]
+    assert np.array_equal(r["U"], a["U"]) and np.array_equal(r["p"], a["p"])

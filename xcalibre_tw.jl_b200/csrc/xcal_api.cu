@@ -51,6 +51,7 @@ struct xcal_ctx_s {
   uint32_t flags = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evrun = nullptr;   // cluster-mode contexts: blocking-sync event for the run wait
   std::string err;
   bool have_mesh = false, have_case = false;
   HostMesh user, mesh;
@@ -79,6 +80,24 @@ struct xcal_ctx_s {
 struct xcal_hmesh_s {
   HostMesh M;
 };
+
+// Host staging buffers.  Ordinary contexts use pinned memory (asynchronous
+// copies).  Cluster-mode contexts (the serving loop) use ordinary heap
+// memory: allocating or freeing pinned memory can wait for work already
+// queued on the device, i.e. for other contexts' runs of several seconds,
+// while pageable copies are staged by the driver without such a wait.
+static cudaError_t stage_alloc(xcal_ctx c, void **p, size_t bytes) {
+  if (c->flags & XCAL_FLAG_CLUSTER) {
+    *p = std::malloc(std::max(bytes, (size_t)1));
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(p, bytes);
+}
+static void stage_free(xcal_ctx c, void *p) {
+  if (!p) return;
+  if (c->flags & XCAL_FLAG_CLUSTER) std::free(p);
+  else cudaFreeHost(p);
+}
 
 static int fail(xcal_ctx c, int code, const std::string &msg) {
   if (c) c->err = msg;
@@ -177,8 +196,14 @@ static void choose_launch_mode(xcal_ctx c, int n) {
   int maxco = max_coresident_blocks(ns, c->occ, c->device);
   if (m && !strcmp(m, "block")) { c->mode = SYNC_BLOCK; c->nblocks = 1; return; }
   if ((c->flags & XCAL_FLAG_CLUSTER) && !m) {   // one hardware cluster: safe beside other kernels
+    // the 4-CTA/SM build once the cluster's CTAs hold more tiles each than
+    // the grid threshold of choose_occ (large cases of a serving stream)
+    const char *o = getenv("XCAL_OCC");
+    const int mc0 = max_cluster_blocks(ns, 0);
+    if (o) c->occ = (atoi(o) == 4 && ns >= 2) ? 1 : 0;
+    else c->occ = (ns >= 2 && ntiles > ((ns == 3) ? 1 : 3) * mc0) ? 1 : 0;
     c->mode = SYNC_CLUSTER;
-    c->nblocks = std::max(1, std::min(max_cluster_blocks(ns), ntiles));
+    c->nblocks = std::max(1, std::min(max_cluster_blocks(ns, c->occ), ntiles));
     return;
   }
   if (m && !strcmp(m, "cluster")) {
@@ -229,6 +254,15 @@ int xcal_ctx_create(int device, uint32_t flags, xcal_ctx *out) {
     return XCAL_ERR_CUDA;
   }
   c->mbuf.stream = c->cbuf.stream = c->rbuf.stream = c->stream;
+  // Contexts of the serving loop wait for their (long) runs asleep: a host
+  // thread spinning in a stream synchronisation for the seconds a case runs
+  // would take a core from the threads setting other cases up.  Short waits
+  // (uploads, read-backs) keep spinning, where a wake-up would cost more.
+  if ((flags & XCAL_FLAG_CLUSTER) &&
+      cudaEventCreateWithFlags(&c->evrun, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess) {
+    delete c;
+    return XCAL_ERR_CUDA;
+  }
   for (auto &e : c->pin_ev)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
       delete c;
@@ -253,10 +287,11 @@ int xcal_ctx_destroy(xcal_ctx c) {
   c->rbuf.release();
   c->cbuf.release();
   c->mbuf.release();
-  if (c->pin) cudaFreeHost(c->pin);
-  if (c->rpin) cudaFreeHost(c->rpin);
+  stage_free(c, c->pin);
+  stage_free(c, c->rpin);
   for (auto &e : c->pin_ev)
     if (e) cudaEventDestroy(e);
+  if (c->evrun) cudaEventDestroy(c->evrun);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -659,9 +694,9 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   CUDA_TRY(c, zero_dev(c, h.bP, sizeof(double) * n));
   if (!c->pin || c->pin_n < (size_t)n * 7) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    if (c->pin) cudaFreeHost(c->pin);
+    stage_free(c, c->pin);
     c->pin = nullptr;
-    CUDA_TRY(c, cudaMallocHost(&c->pin, sizeof(double) * n * 7));
+    CUDA_TRY(c, stage_alloc(c, (void **)&c->pin, sizeof(double) * n * 7));
     c->pin_n = (size_t)n * 7;
   }
   for (bool &b : c->pin_busy) b = false;
@@ -697,7 +732,9 @@ static int field_target(xcal_ctx c, int32_t field, double *&base, int &stride, i
 // (pinned staging, one region per field) and scatter/gather with a small
 // kernel applying the permutation; xcal_field_set returns without waiting
 // for the copy.  Cluster-mode contexts (the serving loop) keep to copy
-// engines only: a kernel could wait for SMs held by other contexts' runs.
+// engines only (a kernel could wait for SMs held by other contexts' runs):
+// the permutation is applied on the host and every copy is contiguous, a
+// vector component by a read-modify-write of the whole interleaved array.
 int xcal_field_set(xcal_ctx c, int32_t field, const double *host, int64_t n) {
   if (!c || !host) return XCAL_ERR_ARG;
   if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_field_set before xcal_case_setup");
@@ -710,10 +747,28 @@ int xcal_field_set(xcal_ctx c, int32_t field, const double *host, int64_t n) {
     CUDA_TRY(c, cudaEventSynchronize(c->pin_ev[field]));
     c->pin_busy[field] = false;
   }
-  if (c->flags & XCAL_FLAG_CLUSTER) {
+  if ((c->flags & XCAL_FLAG_CLUSTER) && stride == 1) {
     for (int64_t i = 0; i < n; ++i) hs[c->perm[i]] = host[i];
-    CUDA_TRY(c, cudaMemcpy2DAsync(base + off, sizeof(double) * stride, hs, sizeof(double), sizeof(double), n,
-                                  cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(base, hs, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  } else if (c->flags & XCAL_FLAG_CLUSTER) {
+    // one component of the interleaved vector array: read-modify-write of the
+    // whole array with contiguous copies (a strided copy moves 8-byte rows)
+    double *hv = c->pin;   // regions of ux, uy, uz: room for n*stride values
+    for (int f = 0; f < 3; ++f)
+      if (c->pin_busy[f]) {
+        CUDA_TRY(c, cudaEventSynchronize(c->pin_ev[f]));
+        c->pin_busy[f] = false;
+      }
+    const size_t bytes = sizeof(double) * (size_t)n * stride;
+    CUDA_TRY(c, cudaMemcpyAsync(hv, base, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (int64_t i = 0; i < n; ++i) hv[(size_t)c->perm[i] * stride + off] = host[i];
+    CUDA_TRY(c, cudaMemcpyAsync(base, hv, bytes, cudaMemcpyHostToDevice, c->stream));
+    for (int f = 0; f < 3; ++f) {
+      CUDA_TRY(c, cudaEventRecord(c->pin_ev[f], c->stream));
+      c->pin_busy[f] = true;
+    }
+    return XCAL_OK;
   } else {
     std::memcpy(hs, host, sizeof(double) * n);
     double *ds = c->d_stage + (size_t)field * n;
@@ -734,10 +789,17 @@ int xcal_field_get(xcal_ctx c, int32_t field, double *host, int64_t n) {
   CUDA_TRY(c, cudaSetDevice(c->device));
   double *hs = c->pin + (size_t)field * n;
   if (c->flags & XCAL_FLAG_CLUSTER) {
-    CUDA_TRY(c, cudaMemcpy2DAsync(hs, sizeof(double), base + off, sizeof(double) * stride, sizeof(double), n,
-                                  cudaMemcpyDeviceToHost, c->stream));
+    // contiguous copy of the whole (interleaved) array, component picked here
+    double *hv = (stride == 1) ? hs : c->pin;
+    if (stride != 1)
+      for (int f = 0; f < 3; ++f)
+        if (c->pin_busy[f]) {
+          CUDA_TRY(c, cudaEventSynchronize(c->pin_ev[f]));
+          c->pin_busy[f] = false;
+        }
+    CUDA_TRY(c, cudaMemcpyAsync(hv, base, sizeof(double) * (size_t)n * stride, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    for (int64_t i = 0; i < n; ++i) host[i] = hs[c->perm[i]];
+    for (int64_t i = 0; i < n; ++i) host[i] = hv[(size_t)c->perm[i] * stride + off];
   } else {
     double *ds = c->d_stage + (size_t)field * n;
     CUDA_TRY(c, launch_field_gather((int)n, base + off, c->d_perm, ds, stride, c->stream));
@@ -782,9 +844,9 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   const size_t need = sizeof(Bar) + 16 + sizeof(double) * nR + sizeof(int) * nK;
   if (!c->rpin || c->rpin_n < need) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    if (c->rpin) cudaFreeHost(c->rpin);
+    stage_free(c, c->rpin);
     c->rpin = nullptr;
-    CUDA_TRY(c, cudaMallocHost(&c->rpin, need));
+    CUDA_TRY(c, stage_alloc(c, &c->rpin, need));
     c->rpin_n = need;
   }
   Bar *hb = (Bar *)c->rpin;
@@ -796,6 +858,10 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   if (iters > 0) {
     CUDA_TRY(c, cudaMemcpyAsync(R, h.R, sizeof(double) * iters * 4, cudaMemcpyDeviceToHost, c->stream));
     if (kry) CUDA_TRY(c, cudaMemcpyAsync(K, h.kry, sizeof(int) * iters * 5, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (c->evrun) {
+    CUDA_TRY(c, cudaEventRecord(c->evrun, c->stream));
+    CUDA_TRY(c, cudaEventSynchronize(c->evrun));
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   float ms = 0.f;

@@ -10,6 +10,6 @@ namespace xcal {
 cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, const KParams *hparams, int prog,
                            int iters, cudaStream_t stream);
 int max_coresident_blocks(int ns, int occ, int device);
-int max_cluster_blocks(int ns);
+int max_cluster_blocks(int ns, int occ = 0);
 const void *program_kernel_ptr(int ns, int mixed, int occ);
 }  // namespace xcal

@@ -2,6 +2,9 @@
 // block, cluster or cooperative grid launch, and the occupancy queries the
 // launch configuration uses.
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "xcal_device.cuh"
 #include "xcal_kernel.h"
@@ -28,6 +31,22 @@ const void *program_kernel_ptr(int ns, int mixed, int occ) {
   return mixed ? program_kernel_f3() : program_kernel_d3();
 }
 
+// Non-portable cluster sizes are allowed once per kernel and device; the
+// attribute is process-wide state, so there is no reason to set it again on
+// every launch (and a serving loop launches from many threads at once).
+static cudaError_t allow_large_clusters(const void *fn) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, bool> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({fn, dev})) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e == cudaSuccess) done[{fn, dev}] = true;
+  return e;
+}
+
 cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, const KParams *hparams, int prog,
                            int iters, cudaStream_t stream) {
   const void *fn = program_kernel_ptr(ns, mixed, occ);
@@ -37,7 +56,7 @@ cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, co
   args[2] = (void *)&iters;
   if (mode == SYNC_BLOCK) return cudaLaunchKernel(fn, dim3(1), dim3(TPB), args, 0, stream);
   if (mode == SYNC_CLUSTER) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaError_t e = allow_large_clusters(fn);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nblocks);
@@ -81,9 +100,33 @@ int max_coresident_blocks(int ns, int occ, int device) {
   return per_sm * sms;
 }
 
-int max_cluster_blocks(int ns) {
-  const void *fn = program_kernel_ptr(ns, 0, 0);
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+static int probe_cluster_blocks(int ns, int occ);
+
+// Largest cluster of the program that fits an empty device, cached per
+// (components, build, device).
+int max_cluster_blocks(int ns, int occ) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    dev = 0;
+  }
+  const std::pair<int, int> key{ns * 4 + occ, dev};
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  const int c = probe_cluster_blocks(ns, occ);
+  std::lock_guard<std::mutex> lk(mu);
+  cache[key] = c;
+  return c;
+}
+
+static int probe_cluster_blocks(int ns, int occ) {
+  const void *fn = program_kernel_ptr(ns, 0, occ);
+  if (allow_large_clusters(fn) != cudaSuccess) {
     (void)cudaGetLastError();
     return 8;
   }
