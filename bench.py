@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, cases/s")
     ap.add_argument("--serve-nmax", type=int, default=400)
     ap.add_argument("--serve-maxit", type=int, default=3000, help="per-case SIMPLE iteration cap")
-    ap.add_argument("--slots", type=int, default=40, help="concurrent serving cases")
+    ap.add_argument("--slots", type=int, default=30,
+                    help="concurrent serving cases (<= 30: one hardware work queue per worker)")
     ap.add_argument("--serve-check", type=int, default=4, help="cases re-run alone for the parity check")
     ap.add_argument("--precision-report", type=int, default=0, metavar="ITERS",
                     help="run ITERS SIMPLE iterations in FP64 and in mixed precision and report the "

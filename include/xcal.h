@@ -282,7 +282,13 @@ int xcal_viscous_force(xcal_ctx ctx, int32_t patch, double rho, double F[3]);
  * threads, each owning a context created with XCAL_FLAG_CLUSTER, so up to
  * `slots` cases run concurrently as separate hardware clusters.  A case runs
  * until every residual is <= tolerance or max_iterations.  The caller's
- * arrays are not referenced after xcal_serve_submit returns. */
+ * arrays are not referenced after xcal_serve_submit returns.
+ * Each worker's stream needs a hardware work queue of its own: the driver
+ * spreads streams round-robin over CUDA_DEVICE_MAX_CONNECTIONS queues (8
+ * unless the environment sets it, 32 at most, read when the process creates
+ * its CUDA context), and a worker whose stream shares a queue with another
+ * worker's run waits behind that whole run for its uploads.  Start the
+ * process with CUDA_DEVICE_MAX_CONNECTIONS=32 and keep slots <= 30. */
 typedef struct xcal_server_s *xcal_server;
 typedef struct {
   int32_t slots;            /* concurrent cases (worker threads), 1..64 */

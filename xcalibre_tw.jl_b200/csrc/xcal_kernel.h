@@ -12,4 +12,5 @@ cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, co
 int max_coresident_blocks(int ns, int occ, int device);
 int max_cluster_blocks(int ns, int occ = 0);
 const void *program_kernel_ptr(int ns, int mixed, int occ);
+void preload_programs();   // load every build on the current device
 }  // namespace xcal

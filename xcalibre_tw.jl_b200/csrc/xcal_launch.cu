@@ -75,6 +75,20 @@ cudaError_t launch_program(int ns, int mixed, int occ, int mode, int nblocks, co
   return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(TPB), args, 0, stream);
 }
 
+// Load every build of the program on the current device now.  With lazy
+// module loading a build is loaded on its first query or launch, and loading
+// can wait for kernels already running on the device; a serving loop, whose
+// runs overlap, loads them all before its first case.
+void preload_programs() {
+  for (int ns = 1; ns <= 3; ++ns)
+    for (int mixed = 0; mixed <= 1; ++mixed)
+      for (int occ = 0; occ <= 1; ++occ) {
+        if (ns == 1 && (mixed || occ)) continue;
+        cudaFuncAttributes a;
+        if (cudaFuncGetAttributes(&a, program_kernel_ptr(ns, mixed, occ)) != cudaSuccess) (void)cudaGetLastError();
+      }
+}
+
 // Occupancy probes: a failed query counts as zero and its error is consumed
 // here, so that it is not reported later by an unrelated call that reads the
 // runtime's last error.

@@ -24,7 +24,13 @@
 #include <thread>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/xcal.h"
+
+namespace xcal {
+void preload_programs();   // xcal_launch.cu
+}
 
 namespace {
 
@@ -178,6 +184,12 @@ int xcal_serve_create(int device, const xcal_serve_cfg *cfg, xcal_server *out) {
   if (cfg->slots < 1 || cfg->slots > 64 || cfg->max_iterations < 1 || !(cfg->tolerance >= 0.0) ||
       cfg->renumber < XCAL_RENUMBER_NONE || cfg->renumber > XCAL_RENUMBER_COLOR)
     return XCAL_ERR_ARG;
+  // load the program's builds before any case runs (see preload_programs)
+  if (cudaSetDevice(device) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return XCAL_ERR_CUDA;
+  }
+  xcal::preload_programs();
   auto *s = new xcal_server_s();
   s->device = device;
   s->cfg = *cfg;

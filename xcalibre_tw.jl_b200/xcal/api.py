@@ -544,7 +544,9 @@ def model2vtk(model, name):
 class Server:
     """A stream of independent cases on one GPU (xcal_serve_*): `slots` worker
     threads, each running its cases as one hardware cluster on its own stream,
-    every case until all residuals are <= tolerance or max_iterations."""
+    every case until all residuals are <= tolerance or max_iterations.
+    slots <= 30 keeps one hardware work queue per worker with the 32 queues
+    the package asks the driver for on import (CUDA_DEVICE_MAX_CONNECTIONS)."""
 
     def __init__(self, device=0, slots=16, max_iterations=3000, tolerance=1e-6,
                  renumber=_abi.RENUMBER_COLOR):
