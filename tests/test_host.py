@@ -52,6 +52,24 @@ def test_serve_config_validation():
     assert lib.xcal_ctx_set_tolerance(None, 1e-6) == -1
 
 
+def test_package_asks_for_one_work_queue_per_serving_worker():
+    """Importing the package asks the driver for 32 hardware work queues (one
+    per serving worker up to 30 slots) and keeps a value the caller has set."""
+    import subprocess
+    import sys
+    pkg = os.path.join(os.path.dirname(__file__), "..", "xcalibre_tw.jl_b200")
+    code = ("import os, sys; sys.path.insert(0, sys.argv[1]); import xcal; "
+            "print(os.environ['CUDA_DEVICE_MAX_CONNECTIONS'])")
+    for preset, want in ((None, "32"), ("4", "4")):
+        env = {k: v for k, v in os.environ.items() if k != "CUDA_DEVICE_MAX_CONNECTIONS"}
+        if preset:
+            env["CUDA_DEVICE_MAX_CONNECTIONS"] = preset
+        out = subprocess.run([sys.executable, "-c", code, pkg], env=env, capture_output=True, text=True,
+                             timeout=300)
+        assert out.returncode == 0, out.stderr
+        assert out.stdout.strip() == want
+
+
 def _has_gpu():
     try:
         import torch
