@@ -47,7 +47,7 @@ def parse():
                     help="concurrent serving cases (<= 30: one hardware work queue per worker)")
     ap.add_argument("--serve-check", type=int, default=4, help="cases re-run alone for the parity check")
     ap.add_argument("--serve-seq", type=int, default=64,
-                    help="first cases of the stream also run one at a time on the whole-GPU path (0: skip)")
+                    help="cases of the stream, evenly spaced, also run one at a time on the whole-GPU path (0: skip)")
     ap.add_argument("--serve-seq-seconds", type=float, default=120.0,
                     help="time bound of the one-at-a-time sample")
     ap.add_argument("--precision-report", type=int, default=0, metavar="ITERS",
@@ -234,7 +234,7 @@ def cpu_model():
 
 # ----------------------------------------------------------------- serving
 def serve_one_at_a_time(a, stream, served):
-    """The same stream's first cases run one at a time on the plain path: one
+    """Every (len/serve_seq)-th case of the same stream run one at a time on the plain path: one
     context per case with the whole-GPU launch (grid barrier over all SMs),
     mixed precision, the same tolerance, cap and stop on a non-finite Krylov
     norm as the serving loop.  Each case is timed from context creation to
@@ -267,7 +267,8 @@ def serve_one_at_a_time(a, stream, served):
 
     one(stream[0])
     t_all, cells_its, same, count = 0.0, 0.0, 0, 0
-    for k in range(min(a.serve_seq, len(stream))):
+    stride = max(1, len(stream) // a.serve_seq)
+    for k in range(0, stride * min(a.serve_seq, len(stream)), stride):
         if t_all > a.serve_seq_seconds:
             break
         t0 = time.perf_counter()
@@ -276,7 +277,7 @@ def serve_one_at_a_time(a, stream, served):
         cells_its += stream[k]["mesh"].ncells * its
         same += int(k in served and served[k]["iterations"] == its)
         count += 1
-    return {"cases": count, "cases_per_s": count / t_all, "cell_iters_per_s": cells_its / t_all,
+    return {"cases": count, "every": stride, "cases_per_s": count / t_all, "cell_iters_per_s": cells_its / t_all,
             "seconds": t_all, "iterations_equal_to_served": same,
             "launch": "whole-GPU grid launch, one case at a time, mixed precision"}
 
@@ -361,8 +362,8 @@ def serve_main(a):
         "one_at_a_time": seq,
         "vs_one_at_a_time": None if not seq else {
             "cases_per_s": value / seq["cases_per_s"], "cell_iters_per_s": cit / seq["cell_iters_per_s"],
-            "note": "cases/s of the whole stream against the first cases run one at a time; cell-iters/s "
-                    "normalises the work of the two samples"},
+            "note": "cases/s of the whole stream against an evenly spaced sample of it run one at a time; "
+                    "cell-iters/s normalises the work of the two samples"},
         "mean_ms": {k: float(np.mean([results[j][k] for j in results])) for k in ("queue_ms", "setup_ms", "run_ms")},
         "parity_sample": check, "clocks": clk.summary(), "impl": "xcal",
     }
