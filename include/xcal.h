@@ -213,15 +213,100 @@ int xcal_simple_run(xcal_ctx ctx, int32_t iterations, double *R_ux, double *R_uy
 /* piso!(model, config; pref): src/Solvers/Solvers_2_PISO.jl:3-238 (2 correctors). */
 int xcal_piso_run(xcal_ctx ctx, int32_t iterations, double *R_ux, double *R_uy,
                   double *R_uz, double *R_p, int32_t *krylov_iters, int32_t *done);
+/* Autotuner (no reference counterpart): times `iterations` SIMPLE iterations
+ * of the context's case in each launch form that computes the same values
+ * (program build for 2 or 4 CTAs per SM, CTA count, hardware cluster or grid
+ * barrier, CG with M^-1 inside its x/r phase), keeps the fastest for the
+ * context, and remembers it for later contexts whose mesh falls in the same
+ * class (components, power-of-two bucket of 256-cell tiles, matrix row width,
+ * precision).  The case's fields are restored afterwards, so the tuning runs
+ * leave no trace in the results.  Environment overrides (XCAL_SYNC, XCAL_OCC,
+ * XCAL_NBLOCKS, XCAL_CG_FUSE) take precedence over a remembered choice. */
+typedef struct {
+  int32_t mode;             /* 1 hardware cluster barrier, 2 grid barrier */
+  int32_t ctas;             /* CTAs of the launch */
+  int32_t ctas_per_sm;      /* build of the program: 2 or 4 resident CTAs per SM */
+  int32_t cg_fused;         /* 1: CG applies M^-1 inside its x/r phase */
+  int32_t candidates;       /* forms timed */
+  int32_t pad;
+  double ms_per_iteration;  /* the chosen form */
+  double ms_default;        /* the form chosen without tuning */
+} xcal_tune_result;
+int xcal_autotune(xcal_ctx ctx, int32_t iterations, xcal_tune_result *out);
+
 /* Device time of the last run, and per-phase device cycle counters when the
- * context was created with XCAL_FLAG_PHASE_TIMERS. */
+ * context was created with XCAL_FLAG_PHASE_TIMERS (zeros otherwise).  The
+ * reference times the whole loop with @time (src/Solvers/Solvers_1_SIMPLE.jl:125);
+ * the timers split a run by phase class: the SM cycles (of the SM running CTA
+ * 0) between the end of one device-wide phase and the end of the next are
+ * charged to the class of the second.  Classes, in array order: */
+enum {
+  XCAL_PH_SETUP = 0,      /* set-up before the loop (interpolate!, flux!, grad!) */
+  XCAL_PH_MOM_ASM,        /* momentum _discretise! + BCs + relaxation + Krylov start (r0 = b - A x0) */
+  XCAL_PH_P_ASM,          /* div! + pressure _discretise! + BCs + setReference! + Krylov start */
+  XCAL_PH_PREC_SETUP,     /* update_preconditioner! level phases and the first M^-1 */
+  XCAL_PH_KRY_SPMV,       /* Krylov phases carrying a SpMV (with the fused vector updates) */
+  XCAL_PH_KRY_PREC,       /* Krylov phases carrying preconditioner sweeps */
+  XCAL_PH_KRY_VEC,        /* Krylov vector/dot-only phases */
+  XCAL_PH_RESID,          /* residual! (+ remove_pressure_source!, H!) */
+  XCAL_PH_FACE,           /* face interpolation phases (interpolate!, correct_boundaries!, flux!) */
+  XCAL_PH_GRAD,           /* Green-Gauss grad! (+ correct_velocity!) */
+  XCAL_PH_UPDATE,         /* run! copy-back and explicit_relaxation! */
+  XCAL_PH_TURB,           /* k-omega phases outside its Krylov solves */
+  XCAL_NPHASES
+};
 int xcal_last_run_stats(xcal_ctx ctx, double *ms, double *phase_cycles, int32_t nphases);
+/* Per-phase cycles and number of phases of each class in the last run. */
+int xcal_last_run_phases(xcal_ctx ctx, int32_t nphases, double *cycles, int64_t *count);
 
 /* Assembled linear systems of the last iteration, in device numbering, CSR order:
  * which = 0 momentum (A shared by ux/uy/uz, b per component), 1 pressure.
  * Mirrors ux_eqn.equation / p_eqn.equation (src/ModelFramework/ModelFramework_0_types.jl:83-89). */
 int xcal_equation_get(xcal_ctx ctx, int32_t which, double *vals, double *b0,
                       double *b1, double *b2);
+
+/* ------------------------------------------------------- operator level
+ * A model equation built by the caller from the reference's operators and
+ * sources (Time, Laplacian, Divergence, Si, Source combined with +, -, ==
+ * and the -> binding to Equation(mesh):
+ * src/ModelFramework/ModelFramework_0_types.jl:15-133 and
+ * ModelFramework_1_operations.jl:3-58), discretised and solved on the
+ * context's mesh.  All arrays are in the context's device numbering (the
+ * mesh of xcal_mesh_export; the caller's own numbering with
+ * XCAL_RENUMBER_NONE).  Matrix values are CSR, in the order of the pattern
+ * xcal_mesh_csr returns (row_ptr/col, 0-based, columns ascending), as
+ * xcal_equation_get returns them. */
+enum { XCAL_TERM_TIME = 0, XCAL_TERM_LAPLACIAN = 1, XCAL_TERM_DIVERGENCE = 2, XCAL_TERM_SI = 3 };
+typedef struct {
+  int32_t kind;         /* XCAL_TERM_* */
+  int32_t scheme;       /* Time: XCAL_TIME_*; Divergence: XCAL_DIV_*; Laplacian: XCAL_LAP_LINEAR; Si: 0 */
+  double sign;          /* +1 or -1, as the operator algebra sets it */
+  const double *flux;   /* face field [nfaces] (Laplacian, Divergence) or cell field [ncells] (Si); NULL for Time */
+} xcal_term;
+typedef struct {
+  double sign;          /* +1 or -1 */
+  const double *field;  /* cell field [ncells] */
+} xcal_source;
+/* discretise!(eqn, prev, runtime) (src/Discretise/Discretise_2_generated_distretisation.jl:5-81,
+ * schemes Discretise_1_schemes.jl:11-113) followed, when nbc > 0, by
+ * apply_boundary_conditions!(eqn, BCs) (Discretise_4_apply_bcs.jl:7-44, functors
+ * Discretise_3_boundary_conditions.jl:4-241); terms in model order.  component
+ * picks the entry of vector BC values; phi (the solved field, cells) is read by
+ * the Si/OmegaWallFunction condition; prev and dt by the Euler term (may be
+ * NULL / 0 otherwise).  vals [nnz] and b [ncells] receive A and b. */
+int xcal_assemble(xcal_ctx ctx, const xcal_term *terms, int32_t nterms, const xcal_source *sources,
+                  int32_t nsources, const xcal_bc *bcs, int32_t nbc, int32_t component, const double *phi,
+                  const double *prev, double dt, double *vals, double *b);
+/* y = A x (SparseArrays mul!, src/Solvers/Solvers_0_functions.jl:18) on the context's pattern. */
+int xcal_spmv(xcal_ctx ctx, const double *vals, const double *x, double *y);
+/* update_preconditioner! then ldiv!(y, P, r) of the DILU preconditioner
+ * (src/Solve/Preconditioners/preconditioners_1_DILU.jl:230-308). */
+int xcal_dilu(xcal_ctx ctx, const double *vals, const double *r, double *y);
+/* grad!(grad_phi) with the Orthogonal scheme (src/Calculate/Calculate_0_gradient.jl:96-112):
+ * face values by interpolate! and correct_boundaries! with the given conditions
+ * (Calculate_2_interpolation.jl:6-148), then green_gauss! (Calculate_1_green_gauss.jl:2-39).
+ * grad [3*ncells]: x, y, z arrays of ncells each, concatenated. */
+int xcal_grad(xcal_ctx ctx, const double *phi, const xcal_bc *bcs, int32_t nbc, double *grad);
 
 /* Standalone linear solve on a caller CSR matrix: run!(eqn, setup) with
  * Krylov.jl solve!(solver, A, b, x0; M=P, itmax, atol, rtol) and the DILU/Jacobi
@@ -246,8 +331,13 @@ int xcal_residual(xcal_ctx ctx, int64_t n, const int32_t *row_ptr, const int32_t
  * xcal_residual, but all pointers are device memory (CSR 0-based, columns
  * ascending; R receives one double) and the partial sums live in a fixed
  * 1 MiB array of the library, so n is limited to 16,777,216 rows
- * (XCAL_ERR_ARG beyond).  The first call on a device resolves that array's
- * address: make it before any stream capture.  The call synchronises the
+ * (XCAL_ERR_ARG beyond).  The arrays must hold n+1 row offsets with
+ * 0 <= d_row_ptr[i] <= d_row_ptr[i+1] <= d_row_ptr[n], and d_row_ptr[n]
+ * column indices and values; the kernel skips (and the call then reports
+ * with XCAL_ERR_ARG) any row range or column index outside those bounds, since
+ * device arrays cannot be checked on the host.  The first call on a device
+ * resolves the library array's address: make it before any stream capture; a
+ * device reset after it is not supported.  The call synchronises the
  * context's stream; calls that overlap on the GPU share the array and race. */
 int xcal_residual_noalloc(xcal_ctx ctx, int64_t n, const int32_t *d_row_ptr, const int32_t *d_col,
                           const double *d_val, const double *d_x, const double *d_b, double *d_R);
@@ -277,25 +367,35 @@ int xcal_viscous_force(xcal_ctx ctx, int32_t patch, double rho, double F[3]);
 
 /* ------------------------------------------------------------- serving
  * A stream of independent cases on one GPU (no reference counterpart: the
- * reference solves one case per process).  Each submitted case is copied
- * (mesh, case, initial fields), then set up and run by one of `slots` worker
- * threads, each owning a context created with XCAL_FLAG_CLUSTER, so up to
- * `slots` cases run concurrently as separate hardware clusters.  A case runs
- * until every residual is <= tolerance or max_iterations.  The caller's
- * arrays are not referenced after xcal_serve_submit returns.
- * Each worker's stream needs a hardware work queue of its own: the driver
- * spreads streams round-robin over CUDA_DEVICE_MAX_CONNECTIONS queues (8
- * unless the environment sets it, 32 at most, read when the process creates
- * its CUDA context), and a worker whose stream shares a queue with another
- * worker's run waits behind that whole run for its uploads.  Start the
- * process with CUDA_DEVICE_MAX_CONNECTIONS=32 and keep slots <= 30. */
+ * reference solves one case per process).  The server runs one persistent
+ * launch for its lifetime; every submitted case is copied (mesh, case,
+ * initial fields), admitted once its device footprint fits the server's
+ * device arena (allocated once at creation, so nothing is allocated on the
+ * device while cases run), laid out on the host by set-up threads, and then
+ * given a group of the launch's CTAs sized by its mesh (ceil(tiles of 256
+ * cells / tiles_per_cta), at most max_ctas) and run to its tolerance or
+ * max_iterations in that group, beside the other cases in flight.  Cases
+ * arriving while others run start as CTAs and memory free up.  Each case's
+ * result is the same as its run alone through xcal_simple_run with the same
+ * precision and tolerance (the device arithmetic does not depend on the CTA
+ * count).  Every case of a server has the mesh dimension `dim` and runs in
+ * `precision` (the case's own precision field is ignored); laminar cases only.
+ * While a server exists its launch holds the GPU: other kernels of the
+ * process wait until xcal_serve_destroy.  The caller's arrays are not
+ * referenced after xcal_serve_submit returns. */
 typedef struct xcal_server_s *xcal_server;
 typedef struct {
-  int32_t slots;            /* concurrent cases (worker threads), 1..64 */
+  int32_t slots;            /* cases running at once, 1..4096 (also bounded by the launch's CTAs) */
   int32_t max_iterations;   /* per-case SIMPLE iteration cap */
   int32_t renumber;         /* XCAL_RENUMBER_* for every case */
-  int32_t pad;
+  int32_t precision;        /* XCAL_PREC_* of every case */
   double tolerance;         /* stop when all residuals <= tolerance */
+  int32_t dim;              /* mesh dimension of every case: 2 or 3 */
+  int32_t tiles_per_cta;    /* CTA group sizing (0: 2) */
+  int32_t max_ctas;         /* largest CTA group of one case (0: 64) */
+  int32_t setup_threads;    /* host threads laying cases out (0: half the cores, 2..8) */
+  double device_bytes;      /* device arena, the admission budget (0: half the free memory) */
+  double host_bytes;        /* pinned host staging for images and results (0: 4 GiB) */
 } xcal_serve_cfg;
 typedef struct {
   int32_t status;           /* XCAL_OK or the failing call's status */
@@ -303,15 +403,18 @@ typedef struct {
   int32_t converged;        /* 1 when the tolerance was reached */
   int32_t ncells;
   double residual[4];       /* last R_ux, R_uy, R_uz, R_p */
-  double queue_ms;          /* submit -> a worker picked the case up */
-  double setup_ms;          /* mesh upload, renumbering, case set-up, fields */
-  double run_ms;            /* device time of the SIMPLE run */
+  double queue_ms;          /* submit -> a set-up thread took the case */
+  double setup_ms;          /* host layout, waiting for arena memory included */
+  double run_ms;            /* case given its CTAs -> results collected */
   double total_ms;          /* submit -> result ready */
 } xcal_serve_result;
 typedef struct {
   int64_t submitted, completed, failed, queued, running;
   double cell_iterations;   /* sum over finished cases of cells x iterations */
-  double run_ms;            /* sum of device run times */
+  double run_ms;            /* sum of run times */
+  double device_bytes;      /* device arena size */
+  double device_bytes_peak; /* most arena memory held by admitted cases at once */
+  int64_t grid_ctas;        /* CTAs of the serving launch */
 } xcal_serve_stats;
 int xcal_serve_create(int device, const xcal_serve_cfg *cfg, xcal_server *out);
 /* U0 holds ux, uy, uz (3 x ncells, the caller's cell order); p0 ncells.
@@ -321,11 +424,13 @@ int xcal_serve_submit(xcal_server s, const xcal_mesh_desc *mesh, const xcal_case
 /* wait_ms: 0 = do not wait, < 0 = wait until done.  Returns XCAL_PENDING while
  * the case runs; once done, fills *res and (when non-NULL) U (3 x ncells) and
  * p (ncells), releases the case and returns XCAL_OK (res->status carries a
- * failed case's error). */
+ * failed case's error: XCAL_ERR_NAN for a case stopped at a non-finite
+ * Krylov residual, XCAL_ERR_OOM for a case larger than the arena,
+ * XCAL_ERR_UNSUPPORTED for a case of another dimension or model). */
 int xcal_serve_poll(xcal_server s, int64_t ticket, int32_t wait_ms, xcal_serve_result *res,
                     double *U, double *p);
 int xcal_serve_stats_get(xcal_server s, xcal_serve_stats *st);
-/* Finishes the running cases, drops the queued ones, joins the workers. */
+/* Finishes the running cases, drops the queued ones, ends the launch. */
 int xcal_serve_destroy(xcal_server s);
 
 #ifdef __cplusplus

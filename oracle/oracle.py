@@ -55,6 +55,12 @@ def lib():
         L.orc_canon_dot.restype = C.c_double
         L.orc_levels.argtypes = [C.c_int64, P_i32, P_i32, P_i32, P_i32]
         L.orc_renumber.argtypes = [vp, C.c_int32, _abi.P_i64]
+        L.orc_last_loop_seconds.argtypes = []
+        L.orc_last_loop_seconds.restype = C.c_double
+        L.orc_assemble.argtypes = [vp, C.POINTER(_abi.Term), C.c_int32, C.POINTER(_abi.Source), C.c_int32,
+                                   C.POINTER(_abi.BC), C.c_int32, C.c_int32, P_d, P_d, C.c_double, P_d, P_d]
+        L.orc_csr_spmv.argtypes = [C.c_int64, P_i32, P_i32, P_d, P_d, P_d]
+        L.orc_grad.argtypes = [vp, P_d, C.POINTER(_abi.BC), C.c_int32, P_d]
         _lib = L
     return _lib
 
@@ -146,7 +152,8 @@ def run(omesh, case, iterations, U, p, k=None, omega=None, nut=None, piso=False,
     if st:
         raise RuntimeError(f"oracle run failed ({st}): {err.value.decode()}")
     out = dict(U=U.reshape(3, n), p=p, k=k, omega=omega, nut=nut, R_ux=R[0], R_uy=R[1],
-               R_uz=R[2], R_p=R[3], krylov=kry.reshape(iterations, 5), done=int(done[0]))
+               R_uz=R[2], R_p=R[3], krylov=kry.reshape(iterations, 5), done=int(done[0]),
+               loop_seconds=float(lib().orc_last_loop_seconds()))
     if want_eqns:
         out.update(AU=AU, bU=bU.reshape(3, n), Ap=Ap, bp=bp)
     return out
@@ -218,3 +225,98 @@ def residual(row_ptr, col, val, x, b):
     bb = np.ascontiguousarray(b, dtype=np.float64)
     return lib().orc_residual(len(bb), _abi.i32ptr(rp), _abi.i32ptr(cl), _abi.dptr(vv), _abi.dptr(xx),
                               _abi.dptr(bb))
+
+
+def renumbered(mesh, mode):
+    """The mesh in the numbering the device uses for `mode` (0 none, 1 RCM,
+    2 colour), built here from the oracle's own permutation (orc_renumber) and
+    numpy, without the product library.  Rules of the renumbered layout:
+    cells in new order; boundary faces keep their ids; internal faces sorted by
+    (lower new owner, higher new owner, old id); every face keeps its owner
+    pair orientation (owners mapped); each cell's face list ordered by new face
+    id (stable); patch faces and cells mapped.  Returns (mesh, perm) with
+    perm[old] = new, 0-based."""
+    om = from_mesh2(mesh)
+    perm = om.renumber(mode) if mode else np.arange(mesh.ncells, dtype=np.int64)
+    if mode == 0:
+        return mesh.copy(), perm
+    nc, nf, nbf = mesh.ncells, mesh.nfaces, mesh.nbfaces
+    inv = np.empty(nc, dtype=np.int64)
+    inv[perm] = np.arange(nc)
+    own = mesh.face_owner.reshape(nf, 2) - 1
+    po = perm[own]
+    fperm = np.arange(nf, dtype=np.int64)
+    if nf > nbf:
+        ids = np.arange(nbf, nf)
+        lo = np.minimum(po[nbf:, 0], po[nbf:, 1])
+        hi = np.maximum(po[nbf:, 0], po[nbf:, 1])
+        order = np.lexsort((ids, hi, lo))
+        fperm[ids[order]] = nbf + np.arange(nf - nbf)
+    finv = np.empty(nf, dtype=np.int64)
+    finv[fperm] = np.arange(nf)
+    m = mesh.copy()
+    m.cell_centre = np.ascontiguousarray(mesh.cell_centre.reshape(nc, 3)[inv].reshape(-1))
+    m.cell_volume = np.ascontiguousarray(mesh.cell_volume[inv])
+    m.face_owner = np.ascontiguousarray((po[finv] + 1).reshape(-1))
+    for k in ("face_centre", "face_normal", "face_e"):
+        setattr(m, k, np.ascontiguousarray(getattr(mesh, k).reshape(nf, 3)[finv].reshape(-1)))
+    for k in ("face_area", "face_delta", "face_weight"):
+        setattr(m, k, np.ascontiguousarray(getattr(mesh, k)[finv]))
+    ptr = mesh.cell_faces_ptr - 1
+    cnt = np.diff(ptr)[inv]
+    nptr = np.concatenate([[0], np.cumsum(cnt)])
+    src = np.repeat(ptr[inv] - nptr[:-1], cnt) + np.arange(nptr[-1])
+    owner_of = np.repeat(np.arange(nc), cnt)
+    newf = fperm[mesh.cell_faces[src] - 1]
+    order = np.lexsort((newf, owner_of))        # stable by new face id inside each cell
+    src = src[order]
+    m.cell_faces_ptr = np.ascontiguousarray(nptr + 1)
+    m.cell_faces = np.ascontiguousarray(fperm[mesh.cell_faces[src] - 1] + 1)
+    m.cell_neighbours = np.ascontiguousarray(perm[mesh.cell_neighbours[src] - 1] + 1)
+    m.cell_nsign = np.ascontiguousarray(mesh.cell_nsign[src])
+    m.patch_faces = np.ascontiguousarray(fperm[mesh.patch_faces - 1] + 1)
+    m.patch_cells = np.ascontiguousarray(perm[mesh.patch_cells - 1] + 1)
+    if m.nnodes > 0:
+        cnp = mesh.cell_nodes_ptr - 1
+        nn = np.diff(cnp)[inv]
+        nnp = np.concatenate([[0], np.cumsum(nn)])
+        m.cell_nodes_ptr = np.ascontiguousarray(nnp + 1)
+        m.cell_nodes = np.ascontiguousarray(mesh.cell_nodes[np.repeat(cnp[inv] - nnp[:-1], nn) + np.arange(nnp[-1])])
+    m._desc = None
+    return m, perm
+
+
+def assemble(omesh, terms, nterms, sources, nsources, bcs, nbc, component=0, phi=None, prev=None, dt=0.0):
+    """Generic discretise! (+ apply_boundary_conditions! with nbc > 0) of a model
+    equation given as ctypes arrays of xcal_term / xcal_source / xcal_bc;
+    returns (CSR values in the pattern's order, b)."""
+    c = omesh.counts()
+    n, tot = int(c[0]), int(c[3])
+    vals = np.zeros(n + tot)
+    b = np.zeros(n)
+    st = lib().orc_assemble(omesh.h, terms, nterms, sources, nsources, bcs, nbc, component,
+                            _abi.dptr(None if phi is None else np.ascontiguousarray(phi, dtype=np.float64)),
+                            _abi.dptr(None if prev is None else np.ascontiguousarray(prev, dtype=np.float64)),
+                            float(dt), _abi.dptr(vals), _abi.dptr(b))
+    if st:
+        raise RuntimeError(f"oracle assemble failed ({st})")
+    return vals, b
+
+
+def csr_spmv(row_ptr, col, val, x):
+    n = len(row_ptr) - 1
+    y = np.zeros(n)
+    lib().orc_csr_spmv(n, _abi.i32ptr(np.ascontiguousarray(row_ptr, dtype=np.int32)),
+                       _abi.i32ptr(np.ascontiguousarray(col, dtype=np.int32)),
+                       _abi.dptr(np.ascontiguousarray(val, dtype=np.float64)),
+                       _abi.dptr(np.ascontiguousarray(x, dtype=np.float64)), _abi.dptr(y))
+    return y
+
+
+def grad(omesh, phi, bcs, nbc):
+    n = int(omesh.counts()[0])
+    g = np.zeros(3 * n)
+    st = lib().orc_grad(omesh.h, _abi.dptr(np.ascontiguousarray(phi, dtype=np.float64)), bcs, nbc, _abi.dptr(g))
+    if st:
+        raise RuntimeError(f"oracle grad failed ({st})")
+    return g.reshape(3, n)

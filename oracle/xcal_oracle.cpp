@@ -51,6 +51,7 @@
 #include <map>
 #include <algorithm>
 #include <limits>
+#include <chrono>
 
 #include "../include/xcal.h"
 
@@ -966,6 +967,98 @@ static void apply_bcs(const OMesh &M, Eqn &E, const Terms &T, const std::vector<
   }
 }
 
+// Generic model equation (a user-built Model of operators and sources, as
+// ModelFramework_1_operations.jl:3-58 builds it): _discretise! with the terms
+// in model order (src/Discretise/Discretise_2_generated_distretisation.jl:5-81,
+// scheme!/scheme_source! of Discretise_1_schemes.jl:11-113), then
+// _apply_boundary_conditions! (Discretise_4_apply_bcs.jl:7-44, functors of
+// Discretise_3_boundary_conditions.jl:4-241) when bcs are given.  Face fields
+// are per face, cell fields per cell, in the mesh's own numbering.
+static void discretise_terms(const OMesh &M, Eqn &E, const xcal_term *terms, int nterms, const xcal_source *srcs,
+                             int nsrc, const double *prev, double dt) {
+  CSC &A = E.A;
+  std::fill(A.nzval.begin(), A.nzval.end(), 0.0);
+  i64 cIndex = 0;
+  for (i64 c = 0; c < M.nc; ++c) {
+    for (i64 k = M.cf_ptr[c]; k < M.cf_ptr[c + 1]; ++k) {
+      const i64 f = M.cf_face[k], nID = M.cf_nbr[k];
+      const double ns = (double)M.cf_sign[k];
+      cIndex = A.pos(c, c);
+      const i64 nIndex = A.pos(c, nID);
+      for (int t = 0; t < nterms; ++t) {
+        const xcal_term &T = terms[t];
+        if (T.kind == XCAL_TERM_LAPLACIAN) {
+          const double ap = T.sign * (-T.flux[f] * M.farea[f]) / M.fdelta[f];
+          A.nzval[cIndex] += ap;
+          A.nzval[nIndex] += -ap;
+        } else if (T.kind == XCAL_TERM_DIVERGENCE && T.scheme == XCAL_DIV_LINEAR) {
+          const V3 xf = M.fcentre[f], xC = M.ccentre[c], xN = M.ccentre[nID];
+          const double weight = vnorm(vsub(xf, xC)) / vnorm(vsub(xN, xC));
+          const double omw = 1.0 - weight;
+          const double ap = T.sign * (T.flux[f] * ns);
+          A.nzval[cIndex] += ap * omw;
+          A.nzval[nIndex] += ap * weight;
+        } else if (T.kind == XCAL_TERM_DIVERGENCE) {
+          const double ap = T.sign * (T.flux[f] * ns);
+          A.nzval[cIndex] += jmax(ap, 0.0);
+          A.nzval[nIndex] += -jmax(-ap, 0.0);
+        }
+      }
+    }
+    if (M.cf_ptr[c + 1] == M.cf_ptr[c]) cIndex = A.pos(c, c);
+    E.b[c] = 0.0;
+    const double volume = M.cvol[c];
+    for (int t = 0; t < nterms; ++t) {
+      const xcal_term &T = terms[t];
+      if (T.kind == XCAL_TERM_TIME && T.scheme == XCAL_TIME_EULER) {
+        const double rdt = 1 / dt;
+        A.nzval[cIndex] += volume * rdt;
+        E.b[c] += prev[c] * volume * rdt;
+      } else if (T.kind == XCAL_TERM_SI) {
+        const double flux = T.sign * T.flux[c] * volume;
+        A.nzval[cIndex] += flux;
+      }
+    }
+    for (int q = 0; q < nsrc; ++q) E.b[c] += srcs[q].sign * srcs[q].field[c] * volume;
+  }
+}
+
+static void apply_bcs_terms(const OMesh &M, Eqn &E, const xcal_term *terms, int nterms, const xcal_bc *bcs, int nbc,
+                            const double *phi, int comp) {
+  CSC &A = E.A;
+  for (int q = 0; q < nbc; ++q) {
+    const xcal_bc &bc = bcs[q];
+    const OPatch &P = M.patches[bc.patch];
+    const double value = bc.value[comp];
+    const bool wall = bc.type == XCAL_BC_NEUMANN || bc.type == XCAL_BC_KWALL || bc.type == XCAL_BC_OMEGAWALL;
+    for (size_t i = 0; i < P.cells.size(); ++i) {
+      const i64 f = P.faces[i], c = P.cells[i];
+      const i64 d = A.pos(c, c);
+      for (int t = 0; t < nterms; ++t) {
+        const xcal_term &T = terms[t];
+        if (T.kind == XCAL_TERM_LAPLACIAN) {
+          if (bc.type == XCAL_BC_DIRICHLET) {
+            const double flux = T.flux[f] * M.farea[f] / M.fdelta[f];
+            const double ap = T.sign * (-flux);
+            A.nzval[d] += ap;
+            E.b[c] += ap * value;
+          }
+        } else if (T.kind == XCAL_TERM_DIVERGENCE && T.scheme == XCAL_DIV_LINEAR) {
+          if (bc.type == XCAL_BC_DIRICHLET) E.b[c] += T.sign * (-T.flux[f] * value);
+          else if (wall) A.nzval[d] += T.sign * (T.flux[f]);
+        } else if (T.kind == XCAL_TERM_DIVERGENCE) {
+          const double ap = T.sign * (T.flux[f]);
+          if (bc.type == XCAL_BC_DIRICHLET) E.b[c] -= ap * value;
+          else if (wall) A.nzval[d] += jmax(ap, 0.0);
+        } else if (T.kind == XCAL_TERM_SI && bc.type == XCAL_BC_OMEGAWALL) {
+          const double flux = T.sign * T.flux[c];
+          E.b[c] += flux * phi[c] * M.cvol[c];
+        }
+      }
+    }
+  }
+}
+
 // implicit_relaxation!, setReference!, explicit_relaxation!: src/Solve/Solve_1_api.jl:48-68
 static void implicit_relaxation(Eqn &E, const std::vector<double> &field, double alpha) {
   for (i64 i = 0; i < E.A.n; ++i) {
@@ -1156,6 +1249,8 @@ struct Run {
   std::vector<xcal_bc> bcU, bcp, bck, bcw, bcn;
 };
 
+static double g_last_loop_seconds = 0.0;   // wall time of the last run's iteration loop
+
 static int run_solver(const OMesh &M, const xcal_case &cfg, bool piso, int iterations, i64 ref_cell,
                       double *Uio, double *pio, double *kio, double *wio, double *nutio,
                       double *R_ux, double *R_uy, double *R_uz, double *R_p, int32_t *kry, int32_t *done,
@@ -1241,6 +1336,7 @@ static int run_solver(const OMesh &M, const xcal_case &cfg, bool piso, int itera
   Vec *Rarr[3] = {nullptr, nullptr, nullptr};
   double *Rout[3] = {R_ux, R_uy, R_uz};
   (void)Rarr;
+  const auto t_loop0 = std::chrono::steady_clock::now();   // the loop alone (set-up excluded)
   for (int iteration = 0; iteration < iterations; ++iteration) {
     it_done = iteration + 1;
     for (int d = 0; d < nU; ++d) {
@@ -1421,6 +1517,7 @@ static int run_solver(const OMesh &M, const xcal_case &cfg, bool piso, int itera
       if (conv) break;
     }
   }
+  g_last_loop_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_loop0).count();
   if (done) *done = it_done;
   for (int d = 0; d < 3; ++d) std::copy(U[d].begin(), U[d].end(), Uio + d * nc);
   std::copy(p.begin(), p.end(), pio);
@@ -1589,6 +1686,74 @@ int orc_run(orc_mesh m, const xcal_case *cfg, int32_t piso, int32_t iterations, 
   if (st && err && nerr) snprintf(err, nerr, "%s", e.c_str());
   return st;
 }
+
+// discretise! (+ apply_boundary_conditions! when nbc > 0) of a user-built model
+// equation on the mesh: vals in CSR (row) order of the mesh's pattern (the
+// pattern arrays of orc_mesh_pattern read as row_ptr/col), b per cell.  comp
+// selects the component of vector BC values.
+int orc_assemble(orc_mesh m, const xcal_term *terms, int32_t nterms, const xcal_source *srcs, int32_t nsrc,
+                 const xcal_bc *bcs, int32_t nbc, int32_t comp, const double *phi, const double *prev, double dt,
+                 double *vals, double *b) {
+  const OMesh &M = m->M;
+  for (int q = 0; q < nbc; ++q)
+    if (bcs[q].patch < 0 || bcs[q].patch >= (int)M.patches.size()) return XCAL_ERR_ARG;
+  Eqn E;
+  build_pattern(M, E.A);
+  E.b.assign(M.nc, 0.0);
+  discretise_terms(M, E, terms, nterms, srcs, nsrc, prev, dt);
+  if (nbc > 0) apply_bcs_terms(M, E, terms, nterms, bcs, nbc, phi, comp);
+  i64 k = 0;   // CSR (row) order of the pattern
+  for (i64 r = 0; r < M.nc; ++r)
+    for (i64 q = E.A.colptr[r]; q < E.A.colptr[r + 1]; ++q) vals[k++] = E.A.get(r, E.A.rowval[q]);
+  std::copy(E.b.begin(), E.b.end(), b);
+  return XCAL_OK;
+}
+
+// CSC of A from its CSR arrays (row_ptr/col 0-based, columns ascending).
+static CSC csc_of_csr(int64_t n, const int32_t *rp, const int32_t *col, const double *val) {
+  CSC A;
+  A.n = n;
+  A.colptr.assign(n + 1, 0);
+  for (i64 i = 0; i < n; ++i) for (int32_t q = rp[i]; q < rp[i + 1]; ++q) A.colptr[col[q] + 1]++;
+  for (i64 j = 0; j < n; ++j) A.colptr[j + 1] += A.colptr[j];
+  A.rowval.assign(A.colptr[n], 0);
+  A.nzval.assign(A.colptr[n], 0.0);
+  std::vector<i64> fill(A.colptr.begin(), A.colptr.end() - 1);
+  for (i64 i = 0; i < n; ++i)
+    for (int32_t q = rp[i]; q < rp[i + 1]; ++q) {
+      const i64 pos = fill[col[q]]++;
+      A.rowval[pos] = i;
+      A.nzval[pos] = val[q];
+    }
+  return A;
+}
+
+// mul!(y, A, x) (CSC column scatter, Solvers_0_functions.jl:18) of a CSR matrix.
+int orc_csr_spmv(int64_t n, const int32_t *rp, const int32_t *col, const double *val, const double *x, double *y) {
+  CSC A = csc_of_csr(n, rp, col, val);
+  std::vector<double> xx(x, x + n), yy(n);
+  spmv(A, xx, yy);
+  std::copy(yy.begin(), yy.end(), y);
+  return XCAL_OK;
+}
+
+// grad!(grad_phi) Orthogonal of a scalar cell field with the given conditions
+// (Calculate_0_gradient.jl:96-112): grad as x, y, z arrays of ncells each.
+int orc_grad(orc_mesh m, const double *phi, const xcal_bc *bcs, int32_t nbc, double *grad) {
+  const OMesh &M = m->M;
+  for (int q = 0; q < nbc; ++q)
+    if (bcs[q].patch < 0 || bcs[q].patch >= (int)M.patches.size()) return XCAL_ERR_ARG;
+  std::vector<xcal_bc> bc(bcs, bcs + nbc);
+  Vec p(phi, phi + M.nc), dx(M.nc), dy(M.nc), dz(M.nc), pf(M.nf);
+  grad_scalar(M, XCAL_GRAD_ORTHOGONAL, dx, dy, dz, pf, p, bc);
+  std::copy(dx.begin(), dx.end(), grad);
+  std::copy(dy.begin(), dy.end(), grad + M.nc);
+  std::copy(dz.begin(), dz.end(), grad + 2 * M.nc);
+  return XCAL_OK;
+}
+
+// Seconds spent in the iteration loop of the last orc_run (its set-up excluded).
+double orc_last_loop_seconds() { return g_last_loop_seconds; }
 
 // run!(eqn) on a CSR matrix (pattern symmetric, columns sorted).
 int orc_linear_solve(int32_t solver, int32_t precon, int64_t n, const int32_t *rp, const int32_t *col,

@@ -1,4 +1,6 @@
+import gzip
 import os
+import shutil
 import sys
 
 import pytest
@@ -7,7 +9,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "xcalibre_tw.jl_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-REFERENCE = "/root/reference"   # present only where the reference is mounted
+# the reference project's own fixtures, copied by tests/golden/reference/copy_fixtures.py
+FIXTURES = os.path.join(ROOT, "tests", "golden", "reference")
 
 
 def pytest_configure(config):
@@ -15,8 +18,11 @@ def pytest_configure(config):
 
 
 @pytest.fixture(scope="session")
-def ref_meshes():
-    d = os.path.join(REFERENCE, "unv_sample_meshes")
-    if not os.path.isdir(d):
-        pytest.skip("reference sample meshes not mounted")
-    return d
+def ref_meshes(tmp_path_factory):
+    """Folder holding the reference's sample UNV meshes (decompressed copies)."""
+    d = tmp_path_factory.mktemp("unv_sample_meshes")
+    for name in os.listdir(FIXTURES):
+        if name.endswith(".unv.gz"):
+            with gzip.open(os.path.join(FIXTURES, name), "rb") as src, open(d / name[:-3], "wb") as dst:
+                shutil.copyfileobj(src, dst)
+    return str(d)

@@ -20,11 +20,16 @@ def rel_l2(a, b):
     return num / den if den > 0 else num
 
 
-def run_device(mesh, model, config, pref, iterations, renumber, piso=False, precision=_abi.PREC_FP64):
+def run_device(mesh, model, config, pref, iterations, renumber, piso=False, precision=_abi.PREC_FP64,
+               tolerance=None, equations=True):
+    """Run on the device; with equations=False only the residual histories,
+    Krylov counts and fields come back (no mesh export or assembled systems)."""
     case, keep = X.make_case(model, config, pref, precision)
     s = X.Solver(mesh, renumber=renumber)
     try:
         s.setup(case)
+        if tolerance is not None:
+            s.set_tolerance(tolerance)
         U, p = cases.fields(model)
         s.set_field(_abi.FIELD_UX, U[0]); s.set_field(_abi.FIELD_UY, U[1]); s.set_field(_abi.FIELD_UZ, U[2])
         s.set_field(_abi.FIELD_P, p)
@@ -38,12 +43,13 @@ def run_device(mesh, model, config, pref, iterations, renumber, piso=False, prec
             out["nut"] = s.get_field(_abi.FIELD_NUT)
         out["U"] = np.stack([s.get_field(_abi.FIELD_UX), s.get_field(_abi.FIELD_UY), s.get_field(_abi.FIELD_UZ)])
         out["p"] = s.get_field(_abi.FIELD_P)
-        out["perm"] = s.permutation() - 1
-        out["dev_mesh"] = s.exported_mesh() if renumber != _abi.RENUMBER_NONE else mesh
-        out["AU"], out["bU"] = s.equation(0)
-        out["Ap"], bp = s.equation(1)
-        out["bp"] = bp[0]
         out["ms"] = s.last_ms()
+        if equations:
+            out["perm"] = s.permutation() - 1
+            out["dev_mesh"] = s.exported_mesh() if renumber != _abi.RENUMBER_NONE else mesh
+            out["AU"], out["bU"] = s.equation(0)
+            out["Ap"], bp = s.equation(1)
+            out["bp"] = bp[0]
     finally:
         s.close()
     return out

@@ -1,12 +1,12 @@
 """Serving loop (xcal_serve_*): a stream of independent cases run concurrently
-on one GPU, each as one hardware cluster on its worker's stream.
+on one GPU inside one persistent launch, each case on a group of its CTAs.
 
 A case's result inside the mix must equal its result run alone through the
 plain path (one context, same precision, same stop tolerance): the device
-program's arithmetic does not depend on the launch form or on other work on
-the GPU, so the comparison is bitwise (iteration count, residual history end,
-fields).  Mixed-precision results are also compared with the FP64 plain path
-(relative L2, reported)."""
+program's arithmetic does not depend on the launch form, the number of CTAs
+or other work on the GPU, so the comparison is bitwise (iteration count,
+residual history end, fields).  Mixed-precision results are also compared
+with the FP64 plain path (relative L2, reported)."""
 import numpy as np
 import pytest
 
@@ -43,9 +43,9 @@ def test_serve_matches_alone(precision):
     # diverges on the coarse BFS meshes from about Re 125 (the CPU oracle
     # does the same), and those cases are covered by the divergence test.
     stream = cases.serving_stream(6, rate=1000.0, seed=7, nmin=16, nmax=48, re_max=60.0)
-    srv = X.Server(slots=4, max_iterations=MAXIT, tolerance=TOL)
+    srv = X.Server(slots=4, max_iterations=MAXIT, tolerance=TOL, precision=precision)
     try:
-        tickets = [srv.submit(c["model"], c["config"], c["pref"], precision) for c in stream]
+        tickets = [srv.submit(c["model"], c["config"], c["pref"]) for c in stream]
         results = [srv.poll(t, wait_ms=-1) for t in tickets]
         st = srv.stats()
     finally:
@@ -103,17 +103,49 @@ def test_serve_stops_a_diverged_case():
     assert st["failed"] == 1 and st["completed"] == 1
 
 
-def test_serve_large_case_matches_alone():
-    """A case with more tiles than three per CTA of its 16-CTA cluster runs on
-    the 4-CTA/SM build of the program inside the serving loop; its result
-    equals the case run alone (grid launch, 2-CTA/SM build) bit for bit."""
+@pytest.mark.parametrize("max_ctas", [1, 7, 64])
+def test_serve_large_case_matches_alone(max_ctas):
+    """A 14,400-cell case (57 tiles) run by groups of 1, 7 and 64 CTAs of the
+    serving launch equals the case run alone (grid launch of the ordinary
+    program) bit for bit."""
     mesh, model, config, pref = cases.cavity2d(120, iterations=1)
     c = dict(mesh=mesh, model=model, config=config, pref=pref)
-    srv = X.Server(slots=1, max_iterations=400, tolerance=TOL)
+    srv = X.Server(slots=1, max_iterations=400, tolerance=TOL, precision=_abi.PREC_FP64, tiles_per_cta=1,
+                   max_ctas=max_ctas)
     try:
-        r = srv.poll(srv.submit(model, config, pref, _abi.PREC_FP64), wait_ms=-1)
+        r = srv.poll(srv.submit(model, config, pref), wait_ms=-1)
     finally:
         srv.close()
     a = _alone(c, _abi.PREC_FP64, maxit=400)
     assert r["status"] == 0 and r["iterations"] == a["done"]
     assert np.array_equal(r["U"], a["U"]) and np.array_equal(r["p"], a["p"])
+
+
+def test_serve_admission_by_footprint():
+    """With a device arena that holds about one case at a time, every case
+    still runs (each waits for the previous one's memory) and the arena's
+    peak use stays within it."""
+    stream = cases.serving_stream(4, rate=1000.0, seed=5, nmin=40, nmax=40, re_max=60.0)
+    srv = X.Server(slots=8, max_iterations=200, tolerance=TOL, precision=_abi.PREC_FP64,
+                   device_bytes=6e6)
+    try:
+        tickets = [srv.submit(c["model"], c["config"], c["pref"]) for c in stream]
+        results = [srv.poll(t, wait_ms=-1) for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert all(r["status"] == 0 for r in results), [r["status"] for r in results]
+    assert st["device_bytes_peak"] <= st["device_bytes"] <= 6e6
+    for c, r in zip(stream, results):
+        a = _alone(c, _abi.PREC_FP64, maxit=200)
+        assert r["iterations"] == a["done"] and np.array_equal(r["p"], a["p"])
+
+
+def test_serve_rejects_a_case_of_another_dimension():
+    srv = X.Server(slots=2, max_iterations=20, tolerance=TOL, precision=_abi.PREC_FP64, dim=2)
+    try:
+        mesh, model, config, pref = cases.cavity3d(6, iterations=1)
+        r = srv.poll(srv.submit(model, config, pref), wait_ms=-1)
+    finally:
+        srv.close()
+    assert r["status"] == -9   # XCAL_ERR_UNSUPPORTED

@@ -26,11 +26,18 @@ INSTANCES = {"d1": (1, "double", 2), "d2": (2, "double", 2), "d3": (3, "double",
              "f3o": (3, "float", 4)}
 UNITS = [("xcal_kernel.cu", tag, ["-DXCAL_INST=" + tag, f"-DXCAL_NS={ns}", f"-DXCAL_T={t}", f"-DXCAL_MB={mb}"])
          for tag, (ns, t, mb) in INSTANCES.items()]
-UNITS += [("xcal_launch.cu", None, []), ("xcal_ops.cu", None, []), ("xcal_api.cu", None, []),
-          ("host_mesh.cpp", None, []), ("xcal_serve.cpp", None, [])]
+# the serving kernel of the 2D and 3D 4-CTA/SM builds, one unit each (compiled in parallel)
+UNITS += [("xcal_kernel.cu", "s" + tag, ["-DXCAL_INST=" + tag, f"-DXCAL_NS={ns}", f"-DXCAL_T={t}",
+                                         f"-DXCAL_MB={mb}", "-DXCAL_SERVE_ONLY"])
+          for tag, (ns, t, mb) in INSTANCES.items() if mb == 4 and ns >= 2]
+UNITS += [("xcal_launch.cu", None, []), ("xcal_ops.cu", None, []), ("xcal_operators.cu", None, []),
+          ("xcal_api.cu", None, []),
+          ("host_mesh.cpp", None, []), ("xcal_serve.cu", None, [])]
 
 
 def build(verbose=False):
+    import time
+    t_start = time.time()   # sources are read from here on; objects are stamped with it
     bdir = os.path.join(HERE, "_build")
     os.makedirs(bdir, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
@@ -50,9 +57,14 @@ def build(verbose=False):
             if verbose:
                 cmd += ["-Xptxas", "-v"]
         procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError("compile failed: " + " ".join(failed[0]))
+    # an object is as new as the sources it was compiled from: a source edited
+    # while the build ran is newer than its object and compiles again next time
     for cmd, p in procs:
-        if p.wait() != 0:
-            raise RuntimeError("compile failed: " + " ".join(cmd))
+        obj = cmd[cmd.index("-o") + 1]
+        os.utime(obj, (t_start, t_start))
     subprocess.run([NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart", "-lpthread"], check=True)
     return OUT
 

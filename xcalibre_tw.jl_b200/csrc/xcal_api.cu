@@ -9,12 +9,16 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
 #include "../../include/xcal.h"
 #include "host_mesh.h"
+#include "xcal_case.h"
 #include "xcal_kernel.h"
 #include "xcal_ops.h"
 
@@ -75,6 +79,8 @@ struct xcal_ctx_s {
   size_t rpin_n = 0;
   std::vector<BcEntry> tabU, tabP;
   std::vector<xcal_bc> bcU_host;   // the case's U conditions (post-processing)
+  unsigned long long *d_phase = nullptr;            // per-phase timers of the last run (device)
+  unsigned long long phase[2 * NPH] = {};           // cycles, counts of the last run
 };
 
 struct xcal_hmesh_s {
@@ -148,6 +154,47 @@ static int upload_c(xcal_ctx c, DevBuf &buf, const T *&dst, const std::vector<T>
     if (s_ != XCAL_OK) return s_; \
   } while (0)
 
+// Sink of an ordinary context: every array is a stream-ordered allocation of
+// the given buffer set, uploaded (blocking) or zero-filled on the context's
+// stream as it is created.
+namespace {
+struct DevSink : Sink {
+  xcal_ctx c;
+  DevBuf &B;
+  int st = XCAL_OK;
+  std::string msg;
+  DevSink(xcal_ctx c_, DevBuf &B_) : c(c_), B(B_) {}
+  char *get(size_t bytes) {
+    char *p = B.alloc<char>(bytes);
+    if (!p && st == XCAL_OK) {
+      st = XCAL_ERR_OOM;
+      msg = "device allocation failed";
+    }
+    return p;
+  }
+  void cuda(cudaError_t e, const char *what) {
+    if (e != cudaSuccess && st == XCAL_OK) {
+      st = XCAL_ERR_CUDA;
+      msg = std::string(what) + ": " + cudaGetErrorString(e);
+    }
+  }
+  void *put(const void *src, size_t bytes) override {
+    char *p = get(bytes);
+    if (p && src && bytes) cuda(copy_sync(c, p, src, bytes, cudaMemcpyHostToDevice), "upload");
+    return p;
+  }
+  void *zeros(size_t bytes) override {
+    char *p = get(bytes);
+    if (p && bytes) cuda(zero_dev(c, p, bytes), "zero fill");
+    return p;
+  }
+  void *scratch(size_t bytes) override { return get(bytes); }
+  bool ok() const override { return st == XCAL_OK; }
+  int error() const override { return st; }
+  std::string message() const override { return msg; }
+};
+}  // namespace
+
 // CG with a two-level DILU can apply M^{-1} inside its x/r phase by
 // recomputing neighbour values (2 instead of 3 grid barriers per iteration,
 // identical results).  On B200 the extra chain of dependent L2 gathers costs
@@ -159,10 +206,60 @@ static int choose_cg_fuse(int ntiles, int nblocks) {
   return f ? atoi(f) != 0 : 0;
 }
 
+// Grid-barrier wait limit and expected extra arrivals, read on every run:
+// XCAL_BARRIER_TIMEOUT_US (default 2 s) bounds one wait; XCAL_BARRIER_EXTRA
+// (default 0) makes every wait expect that many arrivals beyond the launch's
+// CTAs, so that it can end only by its limit (the test of the timeout path).
+static void barrier_knobs(KParams &h) {
+  const char *t = getenv("XCAL_BARRIER_TIMEOUT_US");
+  const char *x = getenv("XCAL_BARRIER_EXTRA");
+  const long long us = t ? atoll(t) : 0;
+  h.bar_timeout_ns = us > 0 ? (unsigned long long)us * 1000ull : 0ull;
+  h.bar_extra = x ? std::max(0, std::min(atoi(x), 1 << 20)) : 0;
+}
+
 static void choose_launch_mode(xcal_ctx c, int n);
+
+// Launch forms chosen by xcal_autotune, per mesh class: (components, tiles
+// bucket = floor(log2 tiles), row width, precision).  A context whose mesh
+// falls in a tuned class starts with the tuned form (the environment
+// overrides of choose_launch_mode still win).  All forms compute the same
+// values; only the time differs.
+struct TuneKey {
+  int ns, bucket, W, prec;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(ns, bucket, W, prec) < std::tie(o.ns, o.bucket, o.W, o.prec);
+  }
+};
+struct TuneChoice {
+  int mode, occ, nblocks, cg_fuse;
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneChoice> g_tune;
+
+static TuneKey tune_key(xcal_ctx c, int prec) {
+  const int ntiles = (c->prep.n + TILE - 1) / TILE;
+  int b = 0;
+  while ((2 << b) <= ntiles) ++b;
+  return TuneKey{c->ns, b, c->prep.W, prec};
+}
+
 static void choose_launch(xcal_ctx c, int n, KParams &h) {
   choose_launch_mode(c, n);
   h.cg_fuse = choose_cg_fuse((n + TILE - 1) / TILE, c->nblocks);
+}
+
+// A tuned form for this context's class, unless the environment forces one.
+static void apply_tuned(xcal_ctx c, int prec) {
+  if (getenv("XCAL_SYNC") || getenv("XCAL_OCC") || getenv("XCAL_NBLOCKS") || getenv("XCAL_CG_FUSE")) return;
+  if (c->flags & XCAL_FLAG_CLUSTER) return;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(c, prec));
+  if (it == g_tune.end()) return;
+  c->mode = it->second.mode;
+  c->occ = it->second.occ;
+  c->nblocks = it->second.nblocks;
+  c->hp.cg_fuse = it->second.cg_fuse;
 }
 
 // Build of the persistent program for a grid launch: the 4-CTA/SM build once
@@ -286,6 +383,7 @@ int xcal_ctx_destroy(xcal_ctx c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->rbuf.release();
   c->cbuf.release();
+  c->d_phase = nullptr;
   c->mbuf.release();
   stage_free(c, c->pin);
   stage_free(c, c->rpin);
@@ -413,55 +511,74 @@ int xcal_hmesh_csr(xcal_hmesh m, int64_t *nnz, int32_t *rp, int32_t *col, int32_
 }
 
 // ------------------------------------------------------------ device mesh
-int xcal_mesh_upload(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
-  if (!c) return XCAL_ERR_ARG;
-  if (renumber < XCAL_RENUMBER_NONE || renumber > XCAL_RENUMBER_COLOR) return fail(c, XCAL_ERR_ARG, "bad renumber mode");
-  CUDA_TRY(c, cudaSetDevice(c->device));
+}  // extern "C"
+
+// Host side of a mesh upload: validation, renumbering, device layout and the
+// launch form; fills the context's mesh, permutation and layout (no device work).
+static int mesh_prepare(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
   std::string e;
-  c->have_mesh = c->have_case = false;
-  c->cbuf.release();
-  c->rbuf.release();
-  c->mbuf.release();
-  c->run_cap = 0;
   int st = mesh_from_desc(d, c->user, e);
   if (st) return fail(c, st, e);
   renumber_perm(c->user, renumber, c->perm);
   apply_perm(c->user, c->perm, renumber != XCAL_RENUMBER_NONE, c->mesh);
   st = prepare(c->mesh, c->prep, e);
   if (st) return fail(c, st, e);
-  const HostMesh &M = c->mesh;
-  const Prep &P = c->prep;
-  c->ns = (M.dim == 3) ? 3 : 2;
+  c->ns = (c->mesh.dim == 3) ? 3 : 2;
   KParams &h = c->hp;
   memset(&h, 0, sizeof(h));
-  h.n = P.n; h.nf = P.nf; h.nbf = P.nbf; h.dim = M.dim; h.ntiles = P.np / TILE;
+  const Prep &P = c->prep;
+  h.n = P.n; h.nf = P.nf; h.nbf = P.nbf; h.dim = c->mesh.dim; h.ntiles = P.np / TILE;
+  h.nfl = P.nfl; h.nbl = P.nbl; h.np = P.np; h.Wf = P.Wf;
+  return XCAL_OK;
+}
+
+// Device arrays of the mesh: geometry (SoA), face lists, boundary lists,
+// level sets and the shared ELL pattern of the matrices.
+static int mesh_arrays(xcal_ctx c, Sink &S) {
+  const HostMesh &M = c->mesh;
+  const Prep &P = c->prep;
+  KParams &h = c->hp;
   std::vector<double> cx(P.n), cy(P.n), cz(P.n), fx(P.nf), fy(P.nf), fz(P.nf), nx(P.nf), ny(P.nf), nz(P.nf);
   for (int i = 0; i < P.n; ++i) { cx[i] = M.cc[3 * i]; cy[i] = M.cc[3 * i + 1]; cz[i] = M.cc[3 * i + 2]; }
   for (int f = 0; f < P.nf; ++f) {
     fx[f] = M.fc[3 * f]; fy[f] = M.fc[3 * f + 1]; fz[f] = M.fc[3 * f + 2];
     nx[f] = M.fn[3 * f]; ny[f] = M.fn[3 * f + 1]; nz[f] = M.fn[3 * f + 2];
   }
-  DevBuf &B = c->mbuf;
-  TRY(upload_c(c, B, h.vol, M.cvol)); TRY(upload_c(c, B, h.ccx, cx)); TRY(upload_c(c, B, h.ccy, cy));
-  TRY(upload_c(c, B, h.ccz, cz)); TRY(upload_c(c, B, h.area, M.farea)); TRY(upload_c(c, B, h.delta, M.fdelta));
-  TRY(upload_c(c, B, h.wgt, M.fweight)); TRY(upload_c(c, B, h.fnx, nx)); TRY(upload_c(c, B, h.fny, ny));
-  TRY(upload_c(c, B, h.fnz, nz)); TRY(upload_c(c, B, h.fcx, fx)); TRY(upload_c(c, B, h.fcy, fy));
-  TRY(upload_c(c, B, h.fcz, fz)); TRY(upload_c(c, B, h.o1, P.o1)); TRY(upload_c(c, B, h.o2, P.o2));
-  TRY(upload_c(c, B, h.f_face, P.f_face)); TRY(upload_c(c, B, h.f_nbr, P.f_nbr));
-  TRY(upload_c(c, B, h.f_pos, P.f_pos)); TRY(upload_c(c, B, h.f_sign, P.f_sign));
-  TRY(upload_c(c, B, h.f_first, P.f_first));
-  TRY(upload_c(c, B, h.cb_ptr, P.cb_ptr)); TRY(upload_c(c, B, h.cb_face, P.cb_face));
-  TRY(upload_c(c, B, h.flev, P.flev)); TRY(upload_c(c, B, h.blev, P.blev));
-  h.nfl = P.nfl; h.nbl = P.nbl; h.np = P.np; h.Wf = P.Wf;
-  const int *ecol, *etpos, *edpos;
-  TRY(upload_c(c, B, ecol, P.e_col)); TRY(upload_c(c, B, etpos, P.e_tpos)); TRY(upload_c(c, B, edpos, P.dpos));
+  h.vol = S.put_v(M.cvol); h.ccx = S.put_v(cx); h.ccy = S.put_v(cy); h.ccz = S.put_v(cz);
+  h.area = S.put_v(M.farea); h.delta = S.put_v(M.fdelta); h.wgt = S.put_v(M.fweight);
+  h.fnx = S.put_v(nx); h.fny = S.put_v(ny); h.fnz = S.put_v(nz);
+  h.fcx = S.put_v(fx); h.fcy = S.put_v(fy); h.fcz = S.put_v(fz);
+  h.o1 = S.put_v(P.o1); h.o2 = S.put_v(P.o2);
+  h.f_face = S.put_v(P.f_face); h.f_nbr = S.put_v(P.f_nbr); h.f_pos = S.put_v(P.f_pos);
+  h.f_sign = S.put_v(P.f_sign); h.f_first = S.put_v(P.f_first);
+  h.cb_ptr = S.put_v(P.cb_ptr); h.cb_face = S.put_v(P.cb_face);
+  h.flev = S.put_v(P.flev); h.blev = S.put_v(P.blev);
+  const int *ecol = S.put_v(P.e_col), *etpos = S.put_v(P.e_tpos), *edpos = S.put_v(P.dpos);
   for (Mat *A : {&h.AU, &h.AP}) { A->col = ecol; A->tpos = etpos; A->dpos = edpos; A->W = P.W; A->np = P.np; }
-  choose_launch(c, P.n, h);
+  if (!S.ok()) return fail(c, S.error(), S.message());
+  return XCAL_OK;
+}
+
+extern "C" {
+
+int xcal_mesh_upload(xcal_ctx c, const xcal_mesh_desc *d, int32_t renumber) {
+  if (!c) return XCAL_ERR_ARG;
+  if (renumber < XCAL_RENUMBER_NONE || renumber > XCAL_RENUMBER_COLOR) return fail(c, XCAL_ERR_ARG, "bad renumber mode");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  c->have_mesh = c->have_case = false;
+  c->cbuf.release();
+  c->d_phase = nullptr;
+  c->rbuf.release();
+  c->mbuf.release();
+  c->run_cap = 0;
+  TRY(mesh_prepare(c, d, renumber));
+  DevSink S(c, c->mbuf);
+  TRY(mesh_arrays(c, S));
+  choose_launch(c, c->prep.n, c->hp);
   {
     std::vector<int> p32(c->perm.begin(), c->perm.end());
-    const int *dp = nullptr;
-    TRY(upload_c(c, B, dp, p32));
-    c->d_perm = const_cast<int *>(dp);
+    c->d_perm = S.put_v(p32);
+    if (!S.ok()) return fail(c, S.error(), S.message());
   }
   c->have_mesh = true;
   return XCAL_OK;
@@ -502,7 +619,7 @@ int xcal_mesh_csr(xcal_ctx c, int64_t *nnz, int32_t *rp, int32_t *col, int32_t *
 }
 
 // -------------------------------------------------------------- case setup
-static int build_bc(xcal_ctx c, DevBuf &B, const xcal_bc *bcs, int nbc, FieldBC &out,
+static int build_bc(xcal_ctx c, Sink &S, const xcal_bc *bcs, int nbc, FieldBC &out,
                     std::vector<BcEntry> &tab, bool vector, const char *what) {
   const HostMesh &M = c->mesh;
   int n = (int)M.nc, nbf = (int)M.nbf;
@@ -540,9 +657,10 @@ static int build_bc(xcal_ctx c, DevBuf &B, const xcal_bc *bcs, int nbc, FieldBC 
       fill[cell]++;
     }
   }
-  TRY(upload_c(c, B, out.tab, tab)); TRY(upload_c(c, B, out.a_ptr, ptr));
-  TRY(upload_c(c, B, out.a_face, face)); TRY(upload_c(c, B, out.a_bc, bcid));
-  TRY(upload_c(c, B, out.fbc, fbc));
+  out.tab = S.put_v(tab); out.a_ptr = S.put_v(ptr);
+  out.a_face = S.put_v(face); out.a_bc = S.put_v(bcid);
+  out.fbc = S.put_v(fbc);
+  if (!S.ok()) return fail(c, S.error(), S.message());
   return XCAL_OK;
 }
 
@@ -575,10 +693,7 @@ static void gmres_alloc(KWorkT<T> &w, int gmax, size_t m, int ns, int nblocks, A
 }
 extern "C" {
 
-int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
-  if (!c || !cfg) return XCAL_ERR_ARG;
-  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_case_setup before xcal_mesh_upload");
-  CUDA_TRY(c, cudaSetDevice(c->device));
+static int check_case(xcal_ctx c, const xcal_case *cfg) {
   if (cfg->model != XCAL_MODEL_LAMINAR && cfg->model != XCAL_MODEL_KOMEGA) return fail(c, XCAL_ERR_ARG, "unknown model");
   const bool turb = (cfg->model == XCAL_MODEL_KOMEGA);
   if (turb) {
@@ -592,12 +707,16 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   TRY(check_solver(c, cfg->solver_p, "p"));
   if (cfg->schemes_U.time == XCAL_TIME_EULER && !(cfg->dt > 0.0)) return fail(c, XCAL_ERR_ARG, "Euler time scheme needs dt > 0");
   if (!(cfg->solver_U.relax > 0.0) || !(cfg->solver_p.relax > 0.0)) return fail(c, XCAL_ERR_ARG, "relaxation factors must be > 0");
-  c->have_case = false;
-  c->cbuf.release();
-  c->rbuf.release();
-  c->run_cap = 0;
+  return XCAL_OK;
+}
+
+// Device arrays of a case (set_solver/set_schemes/@assign! state, equation
+// storage, Krylov work sets, fields).  U0 (3 x n, caller order) and p0 give
+// initial fields; null: zero fields (ScalarField/VectorField constructors),
+// set later through xcal_field_set.
+static int case_arrays(xcal_ctx c, const xcal_case *cfg, Sink &B, const double *U0, const double *p0) {
+  const bool turb = (cfg->model == XCAL_MODEL_KOMEGA);
   KParams &h = c->hp;
-  DevBuf &B = c->cbuf;
   int n = c->prep.n, nf = c->prep.nf, NS = c->ns;
   size_t nnz = (size_t)c->prep.W * c->prep.np;
   TRY(build_bc(c, B, cfg->bc_U, cfg->nbc_U, h.bcU, c->tabU, true, "U"));
@@ -623,12 +742,26 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   h.kU.solver = cfg->solver_U.solver; h.kU.itmax = cfg->solver_U.itmax; h.kU.atol = cfg->solver_U.atol; h.kU.rtol = cfg->solver_U.rtol;
   h.kP.solver = cfg->solver_p.solver; h.kP.itmax = cfg->solver_p.itmax; h.kP.atol = cfg->solver_p.atol; h.kP.rtol = cfg->solver_p.rtol;
   h.AU.precon = cfg->solver_U.preconditioner; h.AP.precon = cfg->solver_p.preconditioner;
-  bool ok = true;
-  auto A = [&](size_t cnt) { double *p = B.alloc<double>(cnt); if (!p) ok = false; return p; };
-  h.AU.val = A(nnz); h.AU.Dpiv = A(n); h.AU.Dinv = A(n);
-  h.AP.val = A(nnz); h.AP.Dpiv = A(n); h.AP.Dinv = A(n);
-  h.U = A((size_t)n * NS); h.Uz2 = A(n); h.p = A(n); h.gp = A((size_t)n * NS); h.bU = A((size_t)n * NS);
-  h.bP = A(n); h.H = A((size_t)n * NS); h.rD = A(n); h.divH = A(n);
+  auto A = [&](size_t cnt) { return B.scratch_n<double>(cnt); };
+  auto Z = [&](size_t cnt) { return B.zeros_n<double>(cnt); };
+  // initial fields in device numbering (interleaved U), or zeros
+  if (U0 && p0) {
+    std::vector<double> u((size_t)n * NS), pp(n), uz(n);
+    for (int i = 0; i < n; ++i) {
+      const int64_t dv = c->perm[i];
+      for (int d = 0; d < NS; ++d) u[(size_t)dv * NS + d] = U0[(size_t)d * n + i];
+      uz[dv] = U0[(size_t)2 * n + i];
+      pp[dv] = p0[i];
+    }
+    h.U = B.put_v(u); h.Uz2 = B.put_v(uz); h.p = B.put_v(pp);
+  } else {
+    h.U = Z((size_t)n * NS); h.Uz2 = Z(n); h.p = Z(n);
+  }
+  h.gp = Z((size_t)n * NS);
+  h.AU.val = Z(nnz); h.AU.Dpiv = A(n); h.AU.Dinv = A(n);
+  h.AP.val = Z(nnz); h.AP.Dpiv = A(n); h.AP.Dinv = A(n);
+  h.bU = Z((size_t)n * NS); h.bP = Z(n);
+  h.H = A((size_t)n * NS); h.rD = A(n); h.divH = A(n);
   h.mdot = A(nf); h.nueff = A(nf); h.rDf = A(nf); h.pf = A(nf); h.UfH = A((size_t)nf * NS);
   for (int k = 0; k < 2; ++k) {
     KWork *w = (k == 0) ? &h.wU : &h.wP;
@@ -653,7 +786,7 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
   gmres_alloc(h.wP, gmP, (size_t)n, 1, c->nblocks, A, gwsP, gRP, allocD);
   h.prec = cfg->precision;
   if (h.prec == XCAL_PREC_MIXED) {
-    auto F = [&](size_t cnt) { float *p = B.alloc<float>(cnt); if (!p) ok = false; return p; };
+    auto F = [&](size_t cnt) { return B.scratch_n<float>(cnt); };
     for (int k = 0; k < 2; ++k) {
       MatT<float> &M32 = (k == 0) ? h.AU32 : h.AP32;
       const Mat &M64 = (k == 0) ? h.AU : h.AP;
@@ -671,27 +804,32 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
     }
   }
   if (turb) {
-    h.k = A(n); h.w = A(n); h.nut = A(n); h.nutf = A(nf); h.nueffk = A(nf); h.nueffw = A(nf);
+    h.k = Z(n); h.w = Z(n); h.nut = Z(n); h.nutf = Z(nf);
+    h.nueffk = A(nf); h.nueffw = A(nf);
     h.Dk = A(n); h.Dw = A(n); h.Pk = A(n); h.Pw = A(n); h.G = A((size_t)n * 9);
   }
-  h.bar = B.alloc<Bar>(1);
-  h.done = B.alloc<int>(1);
-  if (!ok || !h.bar || !h.done) return fail(c, XCAL_ERR_OOM, "device allocation failed");
-  if (turb) {
-    CUDA_TRY(c, zero_dev(c, h.k, sizeof(double) * n));
-    CUDA_TRY(c, zero_dev(c, h.w, sizeof(double) * n));
-    CUDA_TRY(c, zero_dev(c, h.nut, sizeof(double) * n));
-    CUDA_TRY(c, zero_dev(c, h.nutf, sizeof(double) * nf));
-  }
-  // fields start at zero (ScalarField/VectorField constructors)
-  CUDA_TRY(c, zero_dev(c, h.U, sizeof(double) * n * NS));
-  CUDA_TRY(c, zero_dev(c, h.Uz2, sizeof(double) * n));
-  CUDA_TRY(c, zero_dev(c, h.p, sizeof(double) * n));
-  CUDA_TRY(c, zero_dev(c, h.gp, sizeof(double) * n * NS));
-  CUDA_TRY(c, zero_dev(c, h.AU.val, sizeof(double) * nnz));
-  CUDA_TRY(c, zero_dev(c, h.AP.val, sizeof(double) * nnz));
-  CUDA_TRY(c, zero_dev(c, h.bU, sizeof(double) * n * NS));
-  CUDA_TRY(c, zero_dev(c, h.bP, sizeof(double) * n));
+  h.done = B.zeros_n<int>(1);
+  if (!B.ok()) return fail(c, B.error(), B.message());
+  return XCAL_OK;
+}
+
+int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
+  if (!c || !cfg) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_case_setup before xcal_mesh_upload");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  TRY(check_case(c, cfg));
+  c->have_case = false;
+  c->cbuf.release();
+  c->d_phase = nullptr;
+  c->rbuf.release();
+  c->run_cap = 0;
+  KParams &h = c->hp;
+  int n = c->prep.n;
+  apply_tuned(c, cfg->precision);
+  DevSink B(c, c->cbuf);
+  TRY(case_arrays(c, cfg, B, nullptr, nullptr));
+  h.bar = B.scratch_n<Bar>(1);
+  if (!B.ok()) return fail(c, B.error(), B.message());
   if (!c->pin || c->pin_n < (size_t)n * 7) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     stage_free(c, c->pin);
@@ -700,7 +838,7 @@ int xcal_case_setup(xcal_ctx c, const xcal_case *cfg) {
     c->pin_n = (size_t)n * 7;
   }
   for (bool &b : c->pin_busy) b = false;
-  c->d_stage = B.alloc<double>((size_t)n * 7);
+  c->d_stage = c->cbuf.alloc<double>((size_t)n * 7);
   if (!c->d_stage) return fail(c, XCAL_ERR_OOM, "device allocation failed");
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->have_case = true;
@@ -834,6 +972,16 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   h.mode = c->mode;
   h.conv = c->conv;
   h.abort_nan = (c->flags & XCAL_FLAG_ABORT_ON_NAN) ? 1 : 0;
+  barrier_knobs(h);
+  h.phase = nullptr;
+  if (c->flags & XCAL_FLAG_PHASE_TIMERS) {
+    if (!c->d_phase) {
+      c->d_phase = c->cbuf.alloc<unsigned long long>(2 * NPH);
+      if (!c->d_phase) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+    }
+    CUDA_TRY(c, cudaMemsetAsync(c->d_phase, 0, sizeof(unsigned long long) * 2 * NPH, c->stream));
+    h.phase = c->d_phase;
+  }
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
   if (iters > 0)
     CUDA_TRY(c, launch_program(c->ns, h.prec == XCAL_PREC_MIXED, c->occ, c->mode, c->nblocks, &h, prog, iters,
@@ -841,7 +989,8 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   // results: one pinned block, one synchronisation
   const size_t nR = (size_t)std::max(iters, 1) * 4, nK = (size_t)std::max(iters, 1) * 5;
-  const size_t need = sizeof(Bar) + 16 + sizeof(double) * nR + sizeof(int) * nK;
+  const size_t nPh = 2 * NPH;
+  const size_t need = sizeof(Bar) + 16 + sizeof(unsigned long long) * nPh + sizeof(double) * nR + sizeof(int) * nK;
   if (!c->rpin || c->rpin_n < need) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     stage_free(c, c->rpin);
@@ -851,10 +1000,13 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   }
   Bar *hb = (Bar *)c->rpin;
   int *hdn = (int *)((char *)c->rpin + sizeof(Bar));
-  double *R = (double *)((char *)c->rpin + sizeof(Bar) + 16);
+  unsigned long long *hph = (unsigned long long *)((char *)c->rpin + sizeof(Bar) + 16);
+  double *R = (double *)(hph + nPh);
   int *K = (int *)(R + nR);
   CUDA_TRY(c, cudaMemcpyAsync(hb, h.bar, sizeof(Bar), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(hdn, h.done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (h.phase)
+    CUDA_TRY(c, cudaMemcpyAsync(hph, h.phase, sizeof(unsigned long long) * nPh, cudaMemcpyDeviceToHost, c->stream));
   if (iters > 0) {
     CUDA_TRY(c, cudaMemcpyAsync(R, h.R, sizeof(double) * iters * 4, cudaMemcpyDeviceToHost, c->stream));
     if (kry) CUDA_TRY(c, cudaMemcpyAsync(K, h.kry, sizeof(int) * iters * 5, cudaMemcpyDeviceToHost, c->stream));
@@ -869,6 +1021,8 @@ static int run_program(xcal_ctx c, int prog, int32_t iters, double *Rux, double 
   c->last_ms = ms;
   const Bar bar = *hb;
   const int dn = *hdn;
+  if (h.phase) std::copy(hph, hph + nPh, c->phase);
+  else std::fill(c->phase, c->phase + nPh, 0ull);
   for (int i = 0; i < iters; ++i) {
     if (Rux) Rux[i] = R[4 * i];
     if (Ruy) Ruy[i] = R[4 * i + 1];
@@ -893,10 +1047,121 @@ int xcal_piso_run(xcal_ctx c, int32_t iters, double *Rux, double *Ruy, double *R
   return run_program(c, PROG_PISO, iters, Rux, Ruy, Ruz, Rp, kry, done);
 }
 
+// ---------------------------------------------------------------- tuning
+int xcal_autotune(xcal_ctx c, int32_t iters, xcal_tune_result *out) {
+  if (!c || !out) return XCAL_ERR_ARG;
+  if (!c->have_case) return fail(c, XCAL_ERR_STATE, "xcal_autotune before xcal_case_setup");
+  if (iters < 1 || iters > 1000) return fail(c, XCAL_ERR_ARG, "iterations must be 1..1000");
+  if (c->flags & XCAL_FLAG_CLUSTER) return fail(c, XCAL_ERR_STATE, "cluster contexts keep their launch form");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  KParams &h = c->hp;
+  const int n = c->prep.n, NS = c->ns;
+  const int ntiles = (n + TILE - 1) / TILE;
+  const bool gmres = h.wU.gmax > 0 || h.wP.gmax > 0;
+  const int setup_ctas = c->nblocks;   // GMRES per-CTA scratch was sized for this many CTAs
+  struct Cand {
+    int mode, occ, nblocks, cg_fuse;
+  };
+  std::vector<Cand> cands;
+  cands.push_back({c->mode, c->occ, c->nblocks, h.cg_fuse});   // the heuristic's form first
+  auto add = [&](int mode, int occ, int nb, int fuse) {
+    nb = std::max(1, nb);
+    if (gmres && nb > setup_ctas) return;
+    for (const Cand &k : cands)
+      if (k.mode == mode && k.occ == occ && k.nblocks == nb && k.cg_fuse == fuse) return;
+    cands.push_back({mode, occ, nb, fuse});
+  };
+  for (int occ = 0; occ <= (NS >= 2 ? 1 : 0); ++occ) {
+    const int maxco = max_coresident_blocks(NS, occ, c->device);
+    if (maxco < 1) continue;
+    add(SYNC_GRID, occ, std::min(maxco, ntiles), 0);
+    add(SYNC_GRID, occ, std::min(maxco / 2, ntiles), 0);
+  }
+  const int mc = max_cluster_blocks(NS, 0);
+  if (ntiles <= mc) add(SYNC_CLUSTER, 0, ntiles, 0);
+  if (h.kP.solver == XCAL_SOLVER_CG && h.AP.precon == XCAL_PRECON_DILU && h.nfl == 2)
+    add(cands[0].mode, cands[0].occ, cands[0].nblocks, 1 - cands[0].cg_fuse);
+  // fields the runs change, restored before every candidate and at the end
+  DevBuf B;
+  B.stream = c->stream;
+  std::vector<std::pair<double *, size_t>> state = {{h.U, (size_t)n * NS}, {h.p, (size_t)n}};
+  if (h.model == XCAL_MODEL_KOMEGA) {
+    state.push_back({h.k, (size_t)n});
+    state.push_back({h.w, (size_t)n});
+    state.push_back({h.nut, (size_t)n});
+  }
+  std::vector<double *> saved;
+  for (auto &f : state) {
+    double *d = B.alloc<double>(f.second);
+    if (!d) return fail(c, XCAL_ERR_OOM, "device allocation failed");
+    CUDA_TRY(c, cudaMemcpyAsync(d, f.first, sizeof(double) * f.second, cudaMemcpyDeviceToDevice, c->stream));
+    saved.push_back(d);
+  }
+  auto restore = [&]() -> int {
+    for (size_t q = 0; q < state.size(); ++q)
+      CUDA_TRY(c, cudaMemcpyAsync(state[q].first, saved[q], sizeof(double) * state[q].second,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+    return XCAL_OK;
+  };
+  double best = 1e300, first = 0.0;
+  size_t best_k = 0;
+  const double conv = c->conv;
+  c->conv = 0.0;   // time whole iterations: no early stop
+  int st = XCAL_OK;
+  for (size_t k = 0; k < cands.size() && st == XCAL_OK; ++k) {
+    c->mode = cands[k].mode;
+    c->occ = cands[k].occ;
+    c->nblocks = cands[k].nblocks;
+    h.cg_fuse = cands[k].cg_fuse;
+    st = restore();
+    if (st == XCAL_OK) st = run_program(c, PROG_SIMPLE, 1, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (st == XCAL_OK) st = restore();
+    if (st == XCAL_OK) st = run_program(c, PROG_SIMPLE, iters, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (st != XCAL_OK) break;
+    const double ms = c->last_ms / iters;
+    if (k == 0) first = ms;
+    if (ms < best) {
+      best = ms;
+      best_k = k;
+    }
+  }
+  c->conv = conv;
+  const Cand &b = cands[best_k];
+  c->mode = b.mode;
+  c->occ = b.occ;
+  c->nblocks = b.nblocks;
+  h.cg_fuse = b.cg_fuse;
+  const int rs = restore();
+  if (st != XCAL_OK) return st;
+  TRY(rs);
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[tune_key(c, h.prec)] = TuneChoice{b.mode, b.occ, b.nblocks, b.cg_fuse};
+  }
+  out->mode = b.mode;
+  out->ctas = b.nblocks;
+  out->ctas_per_sm = b.occ ? 4 : 2;
+  out->cg_fused = b.cg_fuse;
+  out->candidates = (int32_t)cands.size();
+  out->ms_per_iteration = best;
+  out->ms_default = first;
+  return XCAL_OK;
+}
+
 int xcal_last_run_stats(xcal_ctx c, double *ms, double *phase, int32_t nph) {
   if (!c) return XCAL_ERR_ARG;
   if (ms) *ms = c->last_ms;
-  for (int i = 0; phase && i < nph; ++i) phase[i] = 0.0;
+  for (int i = 0; phase && i < nph; ++i) phase[i] = (i < NPH) ? (double)c->phase[i] : 0.0;
+  return XCAL_OK;
+}
+
+int xcal_last_run_phases(xcal_ctx c, int32_t nph, double *cycles, int64_t *count) {
+  if (!c || nph < 0) return XCAL_ERR_ARG;
+  for (int i = 0; i < nph; ++i) {
+    if (cycles) cycles[i] = (i < NPH) ? (double)c->phase[i] : 0.0;
+    if (count) count[i] = (i < NPH) ? (int64_t)c->phase[NPH + i] : 0;
+  }
   return XCAL_OK;
 }
 
@@ -1031,6 +1296,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
     if (!ok) return fail(c, XCAL_ERR_OOM, "device allocation failed");
   }
   CUDA_TRY(c, cudaMemsetAsync(h.bar, 0, sizeof(Bar), c->stream));
+  barrier_knobs(h);
   CUDA_TRY(c, launch_program(1, 0, 0, mode, nb, &h, PROG_SOLVE, 1, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   Bar bar;
@@ -1041,6 +1307,144 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   if (niter) *niter = (int32_t)so[0];
   if (final_rnorm) *final_rnorm = so[1];
   if (bar.err) return fail(c, XCAL_ERR_TIMEOUT, "device barrier timed out");
+  return XCAL_OK;
+}
+
+// ------------------------------------------------------ operator level
+}  // extern "C"
+
+// The context's ELL values of a CSR matrix on its pattern (xcal_mesh_csr order).
+static void ell_of_csr(xcal_ctx c, const double *vals, std::vector<double> &ell) {
+  const Prep &P = c->prep;
+  ell.assign((size_t)P.W * P.np, 0.0);
+  for (int k = 0; k < P.nnz; ++k) ell[P.csr2ell[k]] = vals[k];
+}
+
+extern "C" {
+
+int xcal_assemble(xcal_ctx c, const xcal_term *terms, int32_t nterms, const xcal_source *sources, int32_t nsources,
+                  const xcal_bc *bcs, int32_t nbc, int32_t comp, const double *phi, const double *prev, double dt,
+                  double *vals, double *b) {
+  if (!c) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_assemble before xcal_mesh_upload");
+  if (!terms || nterms < 1 || nsources < 0 || (nsources > 0 && !sources) || nbc < 0 || (nbc > 0 && !bcs) ||
+      comp < 0 || comp > 2 || !vals || !b)
+    return fail(c, XCAL_ERR_ARG, "bad xcal_assemble arguments");
+  const int n = c->prep.n, nf = c->prep.nf;
+  bool si_wall = false, euler = false;
+  for (int t = 0; t < nterms; ++t) {
+    const xcal_term &T = terms[t];
+    if (T.kind < XCAL_TERM_TIME || T.kind > XCAL_TERM_SI) return fail(c, XCAL_ERR_ARG, "unknown term kind");
+    if (T.kind != XCAL_TERM_TIME && !T.flux) return fail(c, XCAL_ERR_ARG, "term without its flux field");
+    if (T.kind == XCAL_TERM_DIVERGENCE && T.scheme != XCAL_DIV_LINEAR && T.scheme != XCAL_DIV_UPWIND)
+      return fail(c, XCAL_ERR_UNSUPPORTED, "divergence scheme not available");
+    if (T.kind == XCAL_TERM_LAPLACIAN && T.scheme != XCAL_LAP_LINEAR)
+      return fail(c, XCAL_ERR_UNSUPPORTED, "laplacian scheme not available");
+    if (T.kind == XCAL_TERM_TIME && T.scheme == XCAL_TIME_EULER) euler = true;
+    if (T.kind == XCAL_TERM_SI) si_wall = true;
+  }
+  for (int q = 0; q < nsources; ++q)
+    if (!sources[q].field) return fail(c, XCAL_ERR_ARG, "source without its field");
+  if (euler && (!prev || !(dt > 0.0))) return fail(c, XCAL_ERR_ARG, "the Euler term needs prev and dt > 0");
+  if (si_wall && nbc > 0 && !phi) return fail(c, XCAL_ERR_ARG, "the Si term's wall condition needs phi");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  DevBuf B;
+  B.stream = c->stream;
+  DevSink S(c, B);
+  std::vector<OpTerm> dt_(nterms);
+  for (int t = 0; t < nterms; ++t) {
+    const xcal_term &T = terms[t];
+    dt_[t].kind = T.kind;
+    dt_[t].scheme = T.scheme;
+    dt_[t].sign = T.sign;
+    const size_t len = (T.kind == XCAL_TERM_SI) ? n : nf;
+    dt_[t].flux = (T.kind == XCAL_TERM_TIME) ? nullptr : (const double *)S.put(T.flux, sizeof(double) * len);
+  }
+  std::vector<OpSource> ds(std::max(nsources, 1));
+  for (int q = 0; q < nsources; ++q) {
+    ds[q].sign = sources[q].sign;
+    ds[q].field = (const double *)S.put(sources[q].field, sizeof(double) * n);
+  }
+  const OpTerm *dterms = S.put_v(dt_);
+  const OpSource *dsrc = S.put_v(ds);
+  const double *dphi = phi ? (const double *)S.put(phi, sizeof(double) * n) : S.zeros_n<double>(n);
+  const double *dprev = prev ? (const double *)S.put(prev, sizeof(double) * n) : S.zeros_n<double>(n);
+  FieldBC bc{};
+  std::vector<BcEntry> tab;
+  TRY(build_bc(c, S, bcs, nbc, bc, tab, true, "the equation"));
+  double *dval = S.zeros_n<double>((size_t)c->prep.W * c->prep.np);
+  double *db = S.zeros_n<double>(n);
+  if (!S.ok()) return fail(c, S.error(), S.message());
+  CUDA_TRY(c, launch_assemble_terms(c->hp, dterms, nterms, dsrc, nsources, bc, nbc > 0 ? 1 : 0, comp, dphi, dprev,
+                                    dt, dval, db, c->stream));
+  std::vector<double> ell((size_t)c->prep.W * c->prep.np);
+  CUDA_TRY(c, copy_sync(c, ell.data(), dval, sizeof(double) * ell.size(), cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy_sync(c, b, db, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < c->prep.nnz; ++k) vals[k] = ell[c->prep.csr2ell[k]];
+  return XCAL_OK;
+}
+
+int xcal_spmv(xcal_ctx c, const double *vals, const double *x, double *y) {
+  if (!c || !vals || !x || !y) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_spmv before xcal_mesh_upload");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const int n = c->prep.n;
+  std::vector<double> ell;
+  ell_of_csr(c, vals, ell);
+  DevBuf B;
+  B.stream = c->stream;
+  DevSink S(c, B);
+  Mat A = c->hp.AU;
+  A.val = S.put_v(ell);
+  const double *dx = (const double *)S.put(x, sizeof(double) * n);
+  double *dy = S.scratch_n<double>(n);
+  if (!S.ok()) return fail(c, S.error(), S.message());
+  CUDA_TRY(c, launch_spmv(A, n, dx, dy, c->stream));
+  CUDA_TRY(c, copy_sync(c, y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  return XCAL_OK;
+}
+
+int xcal_dilu(xcal_ctx c, const double *vals, const double *r, double *y) {
+  if (!c || !vals || !r || !y) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_dilu before xcal_mesh_upload");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const int n = c->prep.n;
+  std::vector<double> ell;
+  ell_of_csr(c, vals, ell);
+  DevBuf B;
+  B.stream = c->stream;
+  DevSink S(c, B);
+  Mat A = c->hp.AU;
+  A.val = S.put_v(ell);
+  A.Dpiv = S.scratch_n<double>(n);
+  A.Dinv = S.scratch_n<double>(n);
+  A.fval = nullptr;
+  A.precon = XCAL_PRECON_DILU;
+  const double *dr = (const double *)S.put(r, sizeof(double) * n);
+  double *dy = S.zeros_n<double>(n);
+  if (!S.ok()) return fail(c, S.error(), S.message());
+  CUDA_TRY(c, launch_dilu(A, n, c->hp.flev, c->hp.blev, c->hp.nfl, c->hp.nbl, dr, dy, c->stream));
+  CUDA_TRY(c, copy_sync(c, y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  return XCAL_OK;
+}
+
+int xcal_grad(xcal_ctx c, const double *phi, const xcal_bc *bcs, int32_t nbc, double *grad) {
+  if (!c || !phi || !grad || nbc < 0 || (nbc > 0 && !bcs)) return XCAL_ERR_ARG;
+  if (!c->have_mesh) return fail(c, XCAL_ERR_STATE, "xcal_grad before xcal_mesh_upload");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const int n = c->prep.n, nf = c->prep.nf;
+  DevBuf B;
+  B.stream = c->stream;
+  DevSink S(c, B);
+  FieldBC bc{};
+  std::vector<BcEntry> tab;
+  TRY(build_bc(c, S, bcs, nbc, bc, tab, false, "the gradient"));
+  const double *dphi = (const double *)S.put(phi, sizeof(double) * n);
+  double *pf = S.scratch_n<double>(nf);
+  double *dg = S.scratch_n<double>((size_t)3 * n);
+  if (!S.ok()) return fail(c, S.error(), S.message());
+  CUDA_TRY(c, launch_grad(c->hp, bc, dphi, pf, dg, c->stream));
+  CUDA_TRY(c, copy_sync(c, grad, dg, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
   return XCAL_OK;
 }
 
@@ -1096,9 +1500,16 @@ int xcal_residual_noalloc(xcal_ctx c, int64_t n64, const int32_t *d_row_ptr, con
                                      std::to_string(noalloc_max_rows()) + " rows");
   CUDA_TRY(c, cudaSetDevice(c->device));
   double *scratch = nullptr;
-  CUDA_TRY(c, noalloc_scratch(c->device, &scratch));
-  CUDA_TRY(c, launch_residual((int)n64, d_row_ptr, d_col, d_val, d_x, d_b, scratch, d_R, c->stream));
+  int *bad = nullptr;
+  CUDA_TRY(c, noalloc_scratch(c->device, &scratch, &bad));
+  CUDA_TRY(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+  CUDA_TRY(c, launch_residual((int)n64, d_row_ptr, d_col, d_val, d_x, d_b, scratch, d_R, c->stream, bad));
+  int hbad = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (hbad)
+    return fail(c, XCAL_ERR_ARG, std::string("CSR out of bounds:") + ((hbad & 1) ? " row_ptr range" : "") +
+                                     ((hbad & 2) ? " column index" : "") + " (those entries were skipped)");
   return XCAL_OK;
 }
 
@@ -1287,3 +1698,52 @@ int xcal_viscous_force(xcal_ctx c, int32_t patch, double rho, double F[3]) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------- serving images
+namespace xcal {
+
+int build_case_image(const xcal_mesh_desc *mesh, int renumber, const xcal_case *cfg, const double *U0,
+                     const double *p0, double tolerance, int iters, int gmres_ctas, Sink &sink, CaseImage &out,
+                     std::string &err) {
+  if (!mesh || !cfg || !U0 || !p0 || iters < 1 || gmres_ctas < 1) {
+    err = "bad case image arguments";
+    return XCAL_ERR_ARG;
+  }
+  xcal_ctx_s c;   // host-side context: no stream, no device work
+  c.flags = XCAL_FLAG_CLUSTER;
+  int st = mesh_prepare(&c, mesh, renumber);
+  if (st == XCAL_OK) st = check_case(&c, cfg);
+  if (st == XCAL_OK) {
+    c.mode = SYNC_GRID;
+    c.nblocks = gmres_ctas;   // GMRES per-CTA scratch
+    st = mesh_arrays(&c, sink);
+  }
+  if (st == XCAL_OK) st = case_arrays(&c, cfg, sink, U0, p0);
+  if (st != XCAL_OK) {
+    err = c.err;
+    return st;
+  }
+  KParams &h = c.hp;
+  // run arrays: residual histories start at 1.0 as in the reference, Krylov counts at 0
+  std::vector<double> ones((size_t)iters * 4, 1.0);
+  h.R = sink.put_v(ones);
+  h.kry = sink.zeros_n<int>((size_t)iters * 5);
+  if (!sink.ok()) {
+    err = sink.message();
+    return sink.error();
+  }
+  h.conv = tolerance;
+  h.abort_nan = 1;
+  h.mode = SYNC_GRID;
+  h.cg_fuse = 0;
+  h.phase = nullptr;
+  h.bar = nullptr;   // the serving loop gives the case a barrier word when it starts
+  out.prm = h;
+  out.ns = c.ns;
+  out.n = c.prep.n;
+  out.ntiles = h.ntiles;
+  out.perm = c.perm;
+  return XCAL_OK;
+}
+
+}  // namespace xcal

@@ -27,6 +27,9 @@ constexpr int WUNROLL = 8;        // matrix row width handled by the unrolled pa
 enum { SYNC_BLOCK = 0, SYNC_CLUSTER = 1, SYNC_GRID = 2 };
 enum { PROG_SIMPLE = 0, PROG_PISO = 1, PROG_SOLVE = 2 };
 enum { ST_OK = 0, ST_TIMEOUT = 1 };
+// Phase classes of the per-phase timers (XCAL_PH_* in include/xcal.h, same order).
+enum { PH_SETUP = 0, PH_MOM_ASM, PH_P_ASM, PH_PREC_SETUP, PH_KRY_SPMV, PH_KRY_PREC, PH_KRY_VEC, PH_RESID,
+       PH_FACE, PH_GRAD, PH_UPDATE, PH_TURB, NPH };
 
 struct Bar {
   unsigned long long count;
@@ -135,6 +138,54 @@ struct KParams {
   int solve_solver, solve_itmax;
   double solve_atol, solve_rtol;
   double *solve_out;    // [2]: iterations, final rNorm
+  // per-phase timers (XCAL_FLAG_PHASE_TIMERS): CTA 0 accumulates SM cycles and
+  // counts per phase class into phase[0..NPH) and phase[NPH..2NPH); null: off
+  unsigned long long *phase;
+  // grid barrier: wall-clock limit of a wait, and extra arrivals expected
+  // beyond the launch's CTAs (0 in normal use; a test sets 1 so that the wait
+  // can only end by its limit)
+  unsigned long long bar_timeout_ns;
+  int bar_extra;
+};
+
+// Codes of include/xcal.h used on the device.
+enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_KWALL = 2, BC_OMEGAWALL = 3, BC_NUTWALL = 4 };
+enum { DIV_LINEAR = 0, DIV_UPWIND = 1 };
+enum { TIME_STEADY = 0, TIME_EULER = 1 };
+enum { GRAD_ORTHOGONAL = 0, GRAD_MIDPOINT = 1 };
+enum { SOLVER_CG = 0, SOLVER_BICGSTAB = 1, SOLVER_GMRES = 2 };
+enum { PRECON_DILU = 0, PRECON_ILU0 = 4 };
+enum { TERM_TIME = 0, TERM_LAPLACIAN = 1, TERM_DIVERGENCE = 2, TERM_SI = 3 };
+
+// ------------------------------------------------------------------ serving
+// Host <-> serving-kernel records, all in pinned host memory mapped into the
+// device's address space (the host writes jobs and mail, the kernel writes
+// results and state).  A case's device region (arena) is laid out as
+// [copy | zero | scratch]; the CTAs given the case copy the first part from
+// the host image and zero the second before the run.
+struct ServeJob {
+  KParams prm;                     // device pointers into the case's region
+  const uint4 *src;                // host image of the copy part
+  uint4 *dst;                      // start of the case's device region
+  unsigned long long copy16, zero16;   // sizes of the copy and zero parts, in 16-byte units
+  int iters, prog;
+  unsigned *exits;                 // device word: CTAs of the group that left the job (0 between jobs)
+  double *out_U, *out_p;           // results in device numbering: U [n*NS] interleaved, p [n]
+  double *out_R;                   // [iters*4] residual histories (R_ux, R_uy, R_uz, R_p per iteration)
+  int *out_kry;                    // [iters*5] Krylov counts
+  int *out_state;                  // [4]: iterations done, barrier error, non-finite stop, finished (last)
+};
+struct ServeMail {                 // one per CTA of the serving grid
+  unsigned long long seq;          // written last by the host: a new job for this CTA
+  unsigned long long ack;          // written by the CTA when it takes the job
+  ServeJob *job;
+  int vbid, nblk;                  // this CTA's index in the job's group, and the group size
+};
+struct ServeCtl {
+  unsigned shutdown;               // host: leave the serving loop once idle
+  unsigned pad;
+  unsigned long long heartbeat;    // host: advanced while the host side is alive
+  unsigned long long idle_limit_ns;   // an idle CTA leaves after this long without a heartbeat
 };
 
 // ------------------------------------------------------------------ helpers
@@ -170,18 +221,21 @@ __device__ __forceinline__ unsigned long long atom_add_acqrel_u64(unsigned long 
   return old;
 }
 
-constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;   // 2 s
+constexpr unsigned long long BARRIER_TIMEOUT_NS = 2000000000ull;   // 2 s (default limit)
 
 // Barrier over all CTAs of the launch.  The grid form spins with a wall-clock
 // limit: on expiry it records ST_TIMEOUT in bar->err and every CTA returns.
+// A CTA that sees another's error stops waiting as well.
 struct Sync {
   Bar *bar;
   int mode;
   unsigned nb;
+  unsigned extra;                  // arrivals expected beyond the nb CTAs (0)
+  unsigned long long timeout_ns;   // limit of one wait
   unsigned long long epoch;
   int *ok;   // shared flag
 
-  __device__ bool sync() {
+  __device__ __forceinline__ bool sync() {
     if (mode == SYNC_BLOCK) { __syncthreads(); return true; }
     if (mode == SYNC_CLUSTER) {
       __syncthreads();
@@ -192,7 +246,7 @@ struct Sync {
     epoch += 1;
     if (threadIdx.x == 0) {
       int good = 1;
-      const unsigned long long target = epoch * (unsigned long long)nb;
+      const unsigned long long target = epoch * (unsigned long long)nb + extra;
       const unsigned long long v = atom_add_acqrel_u64(&bar->count, 1ull) + 1ull;
       if (v < target) {
         const unsigned long long t0 = globaltimer();
@@ -201,7 +255,7 @@ struct Sync {
           if (ld_acquire_u64(&bar->count) >= target) break;
           if (((++spins) & 63u) == 0u) {
             if (ld_volatile_i32(&bar->err)) { good = 0; break; }
-            if (globaltimer() - t0 > BARRIER_TIMEOUT_NS) {
+            if (globaltimer() - t0 > timeout_ns) {
               atomicExch(&bar->err, ST_TIMEOUT);
               good = 0;
               break;
@@ -296,6 +350,14 @@ __device__ __forceinline__ void load_row(const MatT<T> &A, int i, Row &r) {
   for (int k = 0; k < WUNROLL; ++k) r.c[k] = (k < A.W) ? __ldg(A.col + (size_t)k * A.np + i) : -1;
 }
 
+// Row routines keep their loads out of data-dependent branches: a padding
+// entry (column -1) or an entry the sum skips reads the row's own values
+// instead (always in bounds), and entries past the row width re-read the last
+// entry, so every entry's loads are unconditional and the scheduler may issue
+// those of later entries before the sums of earlier ones.  The sums keep the
+// ascending column order and skip the same entries (by selecting the old
+// partial sum), so the arithmetic is unchanged.
+
 // y = sum_k val[k]*x[col[k]] in ascending column order from 0: the order of
 // SparseArrays' CSC mul! (column scatter) as seen by one row.  GetX(j, d)
 // returns component d of x at row j (it may compute the value on the fly).
@@ -308,10 +370,14 @@ __device__ __forceinline__ void spmv_row(const MatT<T> &A, int i, GetX getx, T (
     load_row(A, i, r);
 #pragma unroll
     for (int k = 0; k < WUNROLL; ++k) {
-      if (r.c[k] >= 0) {
-        const T a = A.val[(size_t)k * A.np + i];
+      const int kk = k < A.W ? k : A.W - 1;
+      const int c = r.c[k];
+      const int j = c >= 0 ? c : i;
+      const T a = A.val[(size_t)kk * A.np + i];
 #pragma unroll
-        for (int d = 0; d < NS; ++d) y[d] = y[d] + a * getx(r.c[k], d);
+      for (int d = 0; d < NS; ++d) {
+        const T t = y[d] + a * getx(j, d);
+        y[d] = (c >= 0) ? t : y[d];
       }
     }
   } else {
@@ -332,16 +398,19 @@ __device__ __forceinline__ void dilu_setup_row(const MatT<T> &A, int i) {
   T D = A.val[__ldg(A.dpos + i)];
   if (A.W <= WUNROLL) {
     // Row entries are in ascending column order, so the lower neighbours are
-    // the entries with 0 <= j < i; all loads are issued before the sums.
+    // the entries with 0 <= j < i.
     Row r;
     load_row(A, i, r);
 #pragma unroll
     for (int k = 0; k < WUNROLL; ++k) {
-      const int j = r.c[k];
-      if (j >= 0 && j < i) {
-        const size_t e = (size_t)k * A.np + i;
-        D = D - A.val[e] * A.val[__ldg(A.tpos + e)] / A.Dpiv[j];
-      }
+      const int kk = k < A.W ? k : A.W - 1;
+      const size_t e = (size_t)kk * A.np + i;
+      const int c = r.c[k];
+      const bool use = c >= 0 && c < i;
+      const int tp = __ldg(A.tpos + e);
+      const int j = use ? c : i;
+      const T t = D - A.val[e] * A.val[use ? tp : (int)e] / A.Dpiv[j];
+      D = use ? t : D;
     }
   } else {
     for (int k = 0; k < A.W; ++k) {
@@ -368,12 +437,15 @@ __device__ __forceinline__ void dilu_fwd_row(const MatT<T> &A, const T (&in)[NS]
     load_row(A, i, r);
 #pragma unroll
     for (int k = 0; k < WUNROLL; ++k) {
-      const int j = r.c[k];
-      if (j >= 0 && j < i) {
-        const size_t e = (size_t)k * A.np + i;
-        const T a = A.val[e], dj = A.Dinv[j];
+      const int kk = k < A.W ? k : A.W - 1;
+      const int c = r.c[k];
+      const bool use = c >= 0 && c < i;
+      const int j = use ? c : i;
+      const T a = A.val[(size_t)kk * A.np + i], dj = A.Dinv[j];
 #pragma unroll
-        for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * dj;
+      for (int d = 0; d < NS; ++d) {
+        const T t = o[d] - a * geto(j, d) * dj;
+        o[d] = use ? t : o[d];
       }
     }
   } else {
@@ -406,11 +478,15 @@ __device__ __forceinline__ void dilu_bwd_row_g(const MatT<T> &A, const T (&out_i
     load_row(A, i, r);
 #pragma unroll
     for (int k = 0; k < WUNROLL; ++k) {
-      const int j = r.c[k];
-      if (j > i) {
-        const T a = A.val[(size_t)k * A.np + i];
+      const int kk = k < A.W ? k : A.W - 1;
+      const int c = r.c[k];
+      const bool use = c > i;
+      const int j = use ? c : i;
+      const T a = A.val[(size_t)kk * A.np + i];
 #pragma unroll
-        for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * di;
+      for (int d = 0; d < NS; ++d) {
+        const T t = o[d] - a * geto(j, d) * di;
+        o[d] = use ? t : o[d];
       }
     }
   } else {
@@ -421,6 +497,119 @@ __device__ __forceinline__ void dilu_bwd_row_g(const MatT<T> &A, const T (&out_i
       const T a = A.val[e];
 #pragma unroll
       for (int d = 0; d < NS; ++d) o[d] = o[d] - a * geto(j, d) * di;
+    }
+  }
+}
+
+// R rows at once (R > 1: the FP32 Krylov phases): the same per-row arithmetic
+// as the single-row routines above, with the loads of all R rows issued
+// together.  Rows of a width above WUNROLL use the single-row routines.
+template <int R, int NS, typename T, class GetX>
+__device__ __forceinline__ void spmv_rows(const MatT<T> &A, const int (&ii)[R], GetX getx, T (&y)[R][NS]) {
+  if (A.W > WUNROLL) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) spmv_row<NS>(A, ii[r], getx, y[r]);
+    return;
+  }
+  Row rw[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    load_row(A, ii[r], rw[r]);
+#pragma unroll
+    for (int d = 0; d < NS; ++d) y[r][d] = T(0);
+  }
+#pragma unroll
+  for (int k = 0; k < WUNROLL; ++k) {
+    const int kk = k < A.W ? k : A.W - 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int c = rw[r].c[k];
+      const int j = c >= 0 ? c : ii[r];
+      const T a = A.val[(size_t)kk * A.np + ii[r]];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        const T t = y[r][d] + a * getx(j, d);
+        y[r][d] = (c >= 0) ? t : y[r][d];
+      }
+    }
+  }
+}
+
+template <int R, int NS, typename T, class GetOut>
+__device__ __forceinline__ void dilu_fwd_rows(const MatT<T> &A, const T (&in)[R][NS], GetOut geto, const int (&ii)[R],
+                                              const int (&bl)[R], T (&o)[R][NS]) {
+  if (A.W > WUNROLL) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) dilu_fwd_row<NS>(A, in[r], geto, ii[r], bl[r], o[r]);
+    return;
+  }
+  Row rw[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    load_row(A, ii[r], rw[r]);
+#pragma unroll
+    for (int d = 0; d < NS; ++d) o[r][d] = in[r][d];
+  }
+#pragma unroll
+  for (int k = 0; k < WUNROLL; ++k) {
+    const int kk = k < A.W ? k : A.W - 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = ii[r], c = rw[r].c[k];
+      const bool use = c >= 0 && c < i;
+      const int j = use ? c : i;
+      const T a = A.val[(size_t)kk * A.np + i], dj = A.Dinv[j];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        const T t = o[r][d] - a * geto(j, d) * dj;
+        o[r][d] = use ? t : o[r][d];
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (bl[r] == 0) {
+      const T di = A.Dinv[ii[r]];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) o[r][d] = o[r][d] * di;
+    }
+}
+
+template <int R, int NS, typename T>
+__device__ __forceinline__ void dilu_bwd_rows(const MatT<T> &A, const T *out, const int (&ii)[R], T (&o)[R][NS]) {
+  if (A.W > WUNROLL) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      T oi[NS];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) oi[d] = out[(size_t)ii[r] * NS + d];
+      dilu_bwd_row_g<NS>(A, oi, [&](int j, int d) { return out[(size_t)j * NS + d]; }, ii[r], o[r]);
+    }
+    return;
+  }
+  Row rw[R];
+  T di[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    load_row(A, ii[r], rw[r]);
+    di[r] = A.Dinv[ii[r]];
+#pragma unroll
+    for (int d = 0; d < NS; ++d) o[r][d] = out[(size_t)ii[r] * NS + d] * di[r];
+  }
+#pragma unroll
+  for (int k = 0; k < WUNROLL; ++k) {
+    const int kk = k < A.W ? k : A.W - 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = ii[r], c = rw[r].c[k];
+      const bool use = c > i;
+      const int j = use ? c : i;
+      const T a = A.val[(size_t)kk * A.np + i];
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        const T t = o[r][d] - a * out[(size_t)j * NS + d] * di[r];
+        o[r][d] = use ? t : o[r][d];
+      }
     }
   }
 }
@@ -538,6 +727,65 @@ __device__ __forceinline__ void diag_precon_setup_row(const MatT<T> &A, int i) {
   } else {
     A.Dinv[i] = T(1);
   }
+}
+
+// ---------------------------------------------------------- face fields
+// interpolate! (Calculate_2_interpolation.jl:112-148) plus correct_boundaries!
+// (:6-110) of a scalar cell field at face f.
+__device__ __forceinline__ double face_scalar(const KParams &P, const double *cellv, int f, const FieldBC &bc,
+                                              bool midpoint) {
+  const int a = __ldg(P.o1 + f), b = __ldg(P.o2 + f);
+  double v;
+  if (midpoint) {
+    v = 0.5 * (cellv[a] + cellv[b]);
+  } else {
+    const double w = __ldg(P.wgt + f);
+    const double omw = 1.0 - w;
+    v = w * cellv[a] + omw * cellv[b];
+  }
+  if (f < P.nbf) {
+    const int bi = __ldg(bc.fbc + f);
+    if (bi >= 0) {
+      const BcEntry &e = bc.tab[bi];
+      v = (e.type == BC_DIRICHLET) ? e.v[0] : cellv[a];
+    }
+  }
+  return v;
+}
+
+// green_gauss! (Calculate_1_green_gauss.jl:2-39) of the face field pf for cell i.
+template <int NS>
+__device__ __forceinline__ void green_gauss_row(const KParams &P, const double *pf, int i, double (&g)[NS]) {
+  double r[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < P.Wf; ++k) {
+    const size_t e = (size_t)k * P.np + i;
+    const int f = __ldg(P.f_face + e);
+    if (f < 0) break;
+    const double ns = (double)__ldg(P.f_sign + e);
+    const double a = __ldg(P.area + f), v = pf[f];
+    r[0] += v * ((a * __ldg(P.fnx + f)) * ns);
+    r[1] += v * ((a * __ldg(P.fny + f)) * ns);
+    if (NS == 3) r[2] += v * ((a * __ldg(P.fnz + f)) * ns);
+  }
+  const double vol = __ldg(P.vol + i);
+#pragma unroll
+  for (int d = 0; d < NS; ++d) r[d] /= vol;
+  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q) {
+    const int f = __ldg(P.cb_face + q);
+    const double a = __ldg(P.area + f), v = pf[f];
+    double bx = v * (a * __ldg(P.fnx + f)), by = v * (a * __ldg(P.fny + f));
+    bx /= vol;
+    by /= vol;
+    r[0] += bx;
+    r[1] += by;
+    if (NS == 3) {
+      double bz = v * (a * __ldg(P.fnz + f));
+      bz /= vol;
+      r[2] += bz;
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < NS; ++d) g[d] = r[d];
 }
 
 }  // namespace xcal

@@ -1,9 +1,13 @@
 // The persistent device program of libxcal: one launch runs `iters` SIMPLE (or
 // PISO) iterations, or one standalone Krylov solve.  Phases are separated by
 // xcal::Sync barriers; every phase is "tile owned" (tile t of 256 rows is always
-// processed by CTA t mod gridDim), so a CTA may reduce over its tiles at the end
-// of a phase sequence without another barrier.  Reference functions are cited at
-// each phase; xcal_device.cuh states the arithmetic contract.
+// processed by CTA t mod the CTA count), so a CTA may reduce over its tiles at
+// the end of a phase sequence without another barrier.  Reference functions are
+// cited at each phase; xcal_device.cuh states the arithmetic contract.
+//
+// A case runs on a group of CTAs numbered 0..vnb()-1 (vbid()): the whole grid
+// of an ordinary launch, or the CTAs the serving kernel (bottom of this file)
+// gives the case.
 #include "xcal_device.cuh"
 #include "xcal_kernel.h"
 
@@ -11,12 +15,11 @@ namespace xcal {
 
 namespace {
 
-enum { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_KWALL = 2, BC_OMEGAWALL = 3, BC_NUTWALL = 4 };
-enum { DIV_LINEAR = 0, DIV_UPWIND = 1 };
-enum { TIME_STEADY = 0, TIME_EULER = 1 };
-enum { GRAD_ORTHOGONAL = 0, GRAD_MIDPOINT = 1 };
-enum { SOLVER_CG = 0, SOLVER_BICGSTAB = 1, SOLVER_GMRES = 2 };
-enum { PRECON_DILU = 0, PRECON_ILU0 = 4 };
+// CTA index within the group running the case, and the group's size.
+__shared__ int s_vbid, s_vnb;
+__device__ __forceinline__ int vbid() { return s_vbid; }
+__device__ __forceinline__ int vnb() { return s_vnb; }
+
 
 // Level-scheduled preconditioners (forward and backward sweeps): DILU, ILU(0).
 template <typename T>
@@ -52,7 +55,23 @@ struct Ctx {
   double *sm;       // [8*MAXK]
   double *sm_out;   // [MAXK]
   double *ws;       // [MAXTL*MAXK*8] staged warp sums
-  __device__ bool sync() { return S.sync(); }
+  // per-phase timers: thread 0 of CTA 0 charges the SM cycles between two
+  // barrier exits to the phase class that was current at the second one
+  bool timers;
+  int tag;
+  long long t_last;
+  unsigned long long *pacc;   // shared [2*NPH]: cycles, counts
+  __device__ __forceinline__ void phase(int t) { tag = t; }
+  __device__ __forceinline__ bool sync() {
+    const bool ok = S.sync();
+    if (timers) {
+      const long long t = clock64();
+      pacc[tag] += (unsigned long long)(t - t_last);
+      pacc[NPH + tag] += 1ull;
+      t_last = t;
+    }
+    return ok;
+  }
 };
 
 template <typename T>
@@ -75,7 +94,7 @@ __device__ __forceinline__ const KWorkT<T> &workP(const KParams &P) {
 // ---------------------------------------------------------------- phases
 template <class F>
 __device__ __forceinline__ void tile_each(const KParams &P, F f) {
-  for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+  for (int t = vbid(); t < P.ntiles; t += vnb()) {
     const int i = t * TILE + threadIdx.x;
     if (i < P.n) f(i);
   }
@@ -89,9 +108,9 @@ __device__ __forceinline__ void tile_each(const KParams &P, F f) {
 template <int K, class F>
 __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
   const KParams &P = *C.P;
-  const int G = gridDim.x, nt = P.ntiles;
+  const int G = vnb(), nt = P.ntiles, B = vbid();
   if (!reduce) {
-    for (int t = blockIdx.x; t < nt; t += G) {
+    for (int t = B; t < nt; t += G) {
       const int i = t * TILE + threadIdx.x;
       double v[K];
       if (i < P.n) f(i, v);
@@ -99,7 +118,7 @@ __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
     return;
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int t0 = blockIdx.x; t0 < nt; t0 += MAXTL * G) {   // chunks of at most MAXTL tiles
+  for (int t0 = B; t0 < nt; t0 += MAXTL * G) {   // chunks of at most MAXTL tiles
     int tl = 0;
     for (int t = t0; t < nt && tl < MAXTL; t += G, ++tl) {
       const int i = t * TILE + threadIdx.x;
@@ -129,9 +148,76 @@ __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
   }
 }
 
+// Rows per thread in the CG phases: two for the FP32 Krylov iterations of the
+// mixed path, one for FP64.  FP32 values move half the bytes per request, so
+// a thread keeps the loads of two rows in flight to reach the memory
+// throughput of the FP64 phases.
+template <typename T>
+struct CgRows {
+  static constexpr int R = (sizeof(T) == 4) ? 2 : 1;
+};
+
+// tile_phase over R tiles at a time: CTA B takes its tiles B, B+G, B+2G, ...
+// R by R, thread t row t of each (ii[r], ok[r] false past the mesh, where
+// ii[r] is a valid row to read from); the per-tile reductions are those of
+// tile_phase (each tile's canonical tree).
+template <int K, int R, class F>
+__device__ __forceinline__ void tile_phase_rows(Ctx &C, bool reduce, F f) {
+  const KParams &P = *C.P;
+  const int G = vnb(), nt = P.ntiles, B = vbid();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int t0 = B; t0 < nt; t0 += MAXTL * G) {
+    int tl = 0;
+    for (int t = t0; t < nt && tl < MAXTL; t += R * G, tl += R) {
+      int ii[R];
+      bool ok[R], tv[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int tr = t + r * G;
+        tv[r] = tr < nt && tl + r < MAXTL;
+        const int i = tr * TILE + threadIdx.x;
+        ok[r] = tv[r] && i < P.n;
+        ii[r] = ok[r] ? i : 0;
+      }
+      double v[R][K];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[r][k] = 0.0;
+      f(ii, ok, v);
+      if (reduce)
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (!tv[r]) continue;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            double x = v[r][k];
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
+            if (lane == 0) C.ws[((tl + r) * K + k) * 8 + wid] = x;
+          }
+        }
+    }
+    if (!reduce) continue;
+    const int ntl = min(MAXTL, (nt - t0 + G - 1) / G);
+    __syncthreads();
+    for (int q = threadIdx.x; q < ntl * K; q += TPB) {
+      const double *w = C.ws + q * 8;
+      double a0 = w[0] + w[4], a1 = w[1] + w[5];
+      const double a2 = w[2] + w[6], a3 = w[3] + w[7];
+      a0 = a0 + a2;
+      a1 = a1 + a3;
+      a0 = a0 + a1;
+      const int k = q % K, t = t0 + (q / K) * G;
+      P.part[(size_t)k * nt + t] = a0;
+    }
+    __syncthreads();
+  }
+}
+
 template <class F>
 __device__ __forceinline__ void grid_each(int count, F f) {
-  for (int i = blockIdx.x * TPB + threadIdx.x; i < count; i += gridDim.x * TPB) f(i);
+  for (int i = vbid() * TPB + threadIdx.x; i < count; i += vnb() * TPB) f(i);
 }
 
 template <int NS>
@@ -191,10 +277,60 @@ __device__ __forceinline__ int precon_tail_phases(const KParams &P, const MatT<T
 // The remaining phases of M^{-1} (in -> out).  With `setup` the DILU pivots
 // (update_preconditioner!) are computed level by level in the same phases.
 // The last phase also computes the K partial sums red(i, v).
-template <int NS, int K, typename T, class Red>
-__device__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *in, T *out, bool setup, int first_lvl, Red red) {
+template <int NS, int K, typename T, class Red, int R = 1>
+__device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *in, T *out, bool setup, int first_lvl, Red red) {
   const KParams &P = *C.P;
   const int nph = precon_tail_phases(P, A, setup, first_lvl);
+  C.phase(setup ? PH_PREC_SETUP : PH_KRY_PREC);
+  if constexpr (R > 1) {
+    if (!setup && A.precon == PRECON_DILU && nph > 0) {
+      // the DILU levels R rows at a time; rows outside the level compute
+      // with what they read and store nothing
+      int ph = 0;
+      for (int l = first_lvl; l < P.nfl; ++l) {
+        const bool last = (++ph == nph);
+        tile_phase_rows<K, R>(C, last, [&](const int (&ii)[R], const bool (&ok)[R], double (&v)[R][K]) {
+          T iv[R][NS], o[R][NS];
+          int bl[R];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            bl[r] = __ldg(P.blev + ii[r]);
+#pragma unroll
+            for (int d = 0; d < NS; ++d) iv[r][d] = in[(size_t)ii[r] * NS + d];
+          }
+          dilu_fwd_rows<R, NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, ii, bl, o);
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            if (ok[r] && __ldg(P.flev + ii[r]) == l)
+#pragma unroll
+              for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
+          if (last)
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              if (ok[r]) red(ii[r], v[r]);
+        });
+        if (!C.sync()) return false;
+      }
+      for (int l = 1; l < P.nbl; ++l) {
+        const bool last = (++ph == nph);
+        tile_phase_rows<K, R>(C, last, [&](const int (&ii)[R], const bool (&ok)[R], double (&v)[R][K]) {
+          T o[R][NS];
+          dilu_bwd_rows<R, NS>(A, out, ii, o);
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            if (ok[r] && __ldg(P.blev + ii[r]) == l)
+#pragma unroll
+              for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
+          if (last)
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              if (ok[r]) red(ii[r], v[r]);
+        });
+        if (!C.sync()) return false;
+      }
+      return true;
+    }
+  }
   if (nph == 0 && setup) {   // nothing left to apply: reduce in a phase of its own
     tile_phase<K>(C, true, [&](int i, double (&v)[K]) { red(i, v); });
     return C.sync();
@@ -290,7 +426,7 @@ __device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A64
 // with the initial dot products (CG: <r,z>; BiCGSTAB: <b,r>, <r,r>), all
 // accumulated in FP64.
 template <int NS, typename T>
-__device__ bool krylov_start(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, int solver) {
+__device__ __forceinline__ bool krylov_start(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, int solver) {
   if (solver != SOLVER_CG) {
     return precon_tail<NS, 2 * NS>(C, A, w.q, w.r[0], true, 1, [&](int i, double (&v)[2 * NS]) {
 #pragma unroll
@@ -319,7 +455,7 @@ __device__ bool krylov_start(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const
 //   G  x += omega*s, r = s - omega*t, reduces <b,r>, <r,r>
 // Vector updates are evaluated in FP64 and stored in T; dots accumulate in FP64.
 template <int NS, typename T>
-__device__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *bb, const KCfg &cfg,
+__device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *bb, const KCfg &cfg,
                          int (&its)[NS], double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   double red[2 * NS];
@@ -355,6 +491,7 @@ __device__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const dou
       return (T)((double)r[k] + beta[d] * pv);
     };
     // A: p update, q = A p, M^{-1} row-local part
+    C.phase(PH_KRY_SPMV);
     tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
       T y[NS], pi[NS], o[NS];
       spmv_row<NS>(A, i, getp, y);
@@ -390,6 +527,7 @@ __device__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const dou
       return (T)((double)r[k] + (-alpha[d]) * (double)vn[k]);
     };
     // D: s, x += alpha p, q = A s, M^{-1} row-local part
+    C.phase(PH_KRY_SPMV);
     tile_phase<2 * NS>(C, tail == 0, [&](int i, double (&v)[2 * NS]) {
       T y[NS], o[NS], si[NS];
 #pragma unroll
@@ -430,6 +568,7 @@ __device__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const dou
     for (int d = 0; d < NS; ++d)
       if (active & (1u << d)) omega[d] = red[2 * d] / red[2 * d + 1];
     // G: x += omega s, r = s - omega t, <b,r>, <r,r>
+    C.phase(PH_KRY_VEC);
     tile_phase<2 * NS>(C, true, [&](int i, double (&v)[2 * NS]) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
@@ -481,7 +620,7 @@ __device__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const dou
 //      neighbours recomputed), backward step of rows without upper neighbours
 //   .. remaining M^-1 phases, the last reduces <r,z>
 template <int NS, typename T>
-__device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg, int (&its)[NS],
+__device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg, int (&its)[NS],
                    double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   const double EPS = 2.220446049250313e-16;
@@ -522,17 +661,38 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
       return (T)((double)z[k] + beta[d] * (double)po[k]);
     };
     // A: p update, q = A p, <p,q>
-    tile_phase<NS>(C, true, [&](int i, double (&v)[NS]) {
-      T y[NS];
-      spmv_row<NS>(A, i, getp, y);
+    C.phase(PH_KRY_SPMV);
+    if constexpr (CgRows<T>::R > 1) {
+      constexpr int R = CgRows<T>::R;
+      tile_phase_rows<NS, R>(C, true, [&](const int (&ii)[R], const bool (&ok)[R], double (&v)[R][NS]) {
+        T y[R][NS];
+        spmv_rows<R, NS>(A, ii, getp, y);
 #pragma unroll
-      for (int d = 0; d < NS; ++d) {
-        const T pi = getp(i, d);
-        if (active & (1u << d)) pn[(size_t)i * NS + d] = pi;
-        v[d] = (double)pi * (double)y[d];
-        w.q[(size_t)i * NS + d] = y[d];
-      }
-    });
+        for (int r = 0; r < R; ++r) {
+          if (!ok[r]) continue;
+          const int i = ii[r];
+#pragma unroll
+          for (int d = 0; d < NS; ++d) {
+            const T pi = getp(i, d);
+            if (active & (1u << d)) pn[(size_t)i * NS + d] = pi;
+            v[r][d] = (double)pi * (double)y[r][d];
+            w.q[(size_t)i * NS + d] = y[r][d];
+          }
+        }
+      });
+    } else {
+      tile_phase<NS>(C, true, [&](int i, double (&v)[NS]) {
+        T y[NS];
+        spmv_row<NS>(A, i, getp, y);
+#pragma unroll
+        for (int d = 0; d < NS; ++d) {
+          const T pi = getp(i, d);
+          if (active & (1u << d)) pn[(size_t)i * NS + d] = pi;
+          v[d] = (double)pi * (double)y[d];
+          w.q[(size_t)i * NS + d] = y[d];
+        }
+      });
+    }
     if (!C.sync()) return false;
     final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
     unsigned upd = 0;
@@ -552,6 +712,47 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
       return (T)((double)ro[k] + (-alpha[d]) * (double)w.q[k]);
     };
     // B: x, r updates and M^{-1} levels 0/1
+    C.phase(PH_KRY_PREC);
+    if constexpr (CgRows<T>::R > 1) {
+      if (A.precon == PRECON_DILU && !fuse) {
+        // R rows at a time; a DILU row of level 0 or 1 is one forward row
+        // (level 0: no lower neighbours, then its diagonal step when it has
+        // no upper ones), the row-local part of precon_local for level 0
+        constexpr int R = CgRows<T>::R;
+        tile_phase_rows<NS, R>(C, tail == 0, [&](const int (&ii)[R], const bool (&ok)[R], double (&v)[R][NS]) {
+          T rr[R][NS], o[R][NS];
+          int fl[R], bl[R];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = ii[r];
+            fl[r] = __ldg(P.flev + i);
+            bl[r] = __ldg(P.blev + i);
+#pragma unroll
+            for (int d = 0; d < NS; ++d) {
+              const size_t k = (size_t)i * NS + d;
+              rr[r][d] = getr(i, d);
+              if (ok[r] && (active & (1u << d))) {
+                w.x[k] = (T)((double)w.x[k] + alpha[d] * (double)pn[k]);
+                rn[k] = rr[r][d];
+              }
+            }
+          }
+          dilu_fwd_rows<R, NS>(A, rr, getr, ii, bl, o);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (!ok[r]) continue;
+            const bool have = fl[r] == 0 || (lvl1 && fl[r] == 1);
+            if (have)
+#pragma unroll
+              for (int d = 0; d < NS; ++d) zw[(size_t)ii[r] * NS + d] = o[r][d];
+            if (tail == 0)
+#pragma unroll
+              for (int d = 0; d < NS; ++d) v[r][d] = (double)rr[r][d] * (double)o[r][d];
+          }
+        });
+        goto phase_b_done;
+      }
+    }
     tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
       T rr[NS], o[NS];
 #pragma unroll
@@ -594,12 +795,15 @@ __device__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg
 #pragma unroll
         for (int d = 0; d < NS; ++d) v[d] = (double)rr[d] * (double)o[d];
     });
+  phase_b_done:
     if (!C.sync()) return false;
-    if (dilu && !fuse && !precon_tail<NS, NS>(C, A, (const T *)rn, zw, false, 2, [&](int i, double (&v)[NS]) {
+    if (dilu && !fuse) {
+      auto rz = [&](int i, double (&v)[NS]) {
 #pragma unroll
-          for (int d = 0; d < NS; ++d) v[d] = (double)rn[(size_t)i * NS + d] * (double)z[(size_t)i * NS + d];
-        }))
-      return false;
+        for (int d = 0; d < NS; ++d) v[d] = (double)rn[(size_t)i * NS + d] * (double)z[(size_t)i * NS + d];
+      };
+      if (!precon_tail<NS, NS, T, decltype(rz), CgRows<T>::R>(C, A, (const T *)rn, zw, false, 2, rz)) return false;
+    }
     final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
     unsigned cont = 0;
 #pragma unroll
@@ -667,7 +871,7 @@ __device__ __forceinline__ void sym_givens(double a, double b, double &c, double
 }
 
 template <int NS, typename T>
-__device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg, int (&its)[NS],
+__device__ __forceinline__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &cfg, int (&its)[NS],
                       double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   const double BTOL = 1.8189894035458565e-12;   // eps(Float64)^(3/4) = 2^-39
@@ -675,7 +879,7 @@ __device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &
   final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
   const int G1 = w.gmax + 1;
   const int kmax = min(cfg.itmax, w.gmax);
-  double *gws = w.gws + (size_t)blockIdx.x * NS * 4 * G1;
+  double *gws = w.gws + (size_t)vbid() * NS * 4 * G1;
   const size_t rs = (size_t)w.gmax * (w.gmax + 1) / 2;
   double beta0[NS], rnorm[NS], eps[NS], hbis[NS];
   unsigned active = 0;
@@ -710,6 +914,7 @@ __device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &
     for (int d = 0; d < NS; ++d) div[d] = (k == 1) ? beta0[d] : hbis[d];
     auto getv = [&](int j, int d) -> T { return (T)((double)src[(size_t)j * NS + d] / div[d]); };
     // P1: V_k, t = A V_k, M^{-1} row-local part
+    C.phase(PH_KRY_SPMV);
     tile_phase<NS>(C, tail == 0, [&](int i, double (&v)[NS]) {
       T y[NS], o[NS], vk[NS];
       spmv_row<NS>(A, i, getv, y);
@@ -746,6 +951,7 @@ __device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &
       const T *Vp = w.V + (size_t)(m - 2) * nv;
       const T *Vm = w.V + (size_t)(m - 1) * nv;
       const bool norm = (m == k + 1);
+      C.phase(PH_KRY_VEC);
       tile_phase<NS>(C, true, [&](int i, double (&v)[NS]) {
 #pragma unroll
         for (int d = 0; d < NS; ++d) {
@@ -783,7 +989,7 @@ __device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &
         zz[k - 1] = c_ * zz[k - 1];
         zz[k] = zeta;
         C.sm_out[d] = fabs(zeta);
-        if (blockIdx.x == 0) {
+        if (vbid() == 0) {
           double *Rc = w.gR + (size_t)d * rs + (size_t)(k - 1) * k / 2;
           for (int i = 0; i < k; ++i) Rc[i] = col[i];
         }
@@ -807,6 +1013,7 @@ __device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &
   }
   if (ran) {
     // R complete (CTA 0's stores) after this barrier; y by back substitution
+    C.phase(PH_KRY_VEC);
     if (!C.sync()) return false;
     if (threadIdx.x == 0) {
 #pragma unroll
@@ -844,7 +1051,7 @@ __device__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const KCfg &
 }
 
 template <int NS, typename T>
-__device__ bool krylov(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, const KCfg &cfg,
+__device__ __forceinline__ bool krylov(Ctx &C, const MatT<T> &A, const KWorkT<T> &w, const double *b, const KCfg &cfg,
                        int solver, int (&its)[NS], double (&rn)[NS]) {
   if (solver == SOLVER_BICGSTAB) return bicgstab<NS, T>(C, A, w, b, cfg, its, rn);
   if (solver == SOLVER_GMRES) return gmres<NS, T>(C, A, w, cfg, its, rn);
@@ -1043,27 +1250,6 @@ __device__ __forceinline__ void face_vector(const KParams &P, const double *cell
   }
 }
 
-__device__ __forceinline__ double face_scalar(const KParams &P, const double *cellv, int f, const FieldBC &bc,
-                                              bool midpoint) {
-  const int a = __ldg(P.o1 + f), b = __ldg(P.o2 + f);
-  double v;
-  if (midpoint) {
-    v = 0.5 * (cellv[a] + cellv[b]);
-  } else {
-    const double w = __ldg(P.wgt + f);
-    const double omw = 1.0 - w;
-    v = w * cellv[a] + omw * cellv[b];
-  }
-  if (f < P.nbf) {
-    const int bi = __ldg(bc.fbc + f);
-    if (bi >= 0) {
-      const BcEntry &e = bc.tab[bi];
-      v = (e.type == BC_DIRICHLET) ? e.v[0] : cellv[a];
-    }
-  }
-  return v;
-}
-
 // flux!(mdotf, Uf) (Solvers_0_functions.jl:65-73) from the face-interpolated U.
 template <int NS>
 __device__ __forceinline__ void face_mdot(const KParams &P, int f) {
@@ -1076,41 +1262,6 @@ __device__ __forceinline__ void face_mdot(const KParams &P, int f) {
   double m = u[0] * (a * __ldg(P.fnx + f)) + u[1] * (a * __ldg(P.fny + f));
   if (NS == 3) m = m + u[2] * (a * __ldg(P.fnz + f));
   P.mdot[f] = m;
-}
-
-// green_gauss! (Calculate_1_green_gauss.jl:2-39) of the face field pf for cell i.
-template <int NS>
-__device__ __forceinline__ void green_gauss_row(const KParams &P, const double *pf, int i, double (&g)[NS]) {
-  double r[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < P.Wf; ++k) {
-    const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
-    if (f < 0) break;
-    const double ns = (double)__ldg(P.f_sign + e);
-    const double a = __ldg(P.area + f), v = pf[f];
-    r[0] += v * ((a * __ldg(P.fnx + f)) * ns);
-    r[1] += v * ((a * __ldg(P.fny + f)) * ns);
-    if (NS == 3) r[2] += v * ((a * __ldg(P.fnz + f)) * ns);
-  }
-  const double vol = __ldg(P.vol + i);
-#pragma unroll
-  for (int d = 0; d < NS; ++d) r[d] /= vol;
-  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q) {
-    const int f = __ldg(P.cb_face + q);
-    const double a = __ldg(P.area + f), v = pf[f];
-    double bx = v * (a * __ldg(P.fnx + f)), by = v * (a * __ldg(P.fny + f));
-    bx /= vol;
-    by /= vol;
-    r[0] += bx;
-    r[1] += by;
-    if (NS == 3) {
-      double bz = v * (a * __ldg(P.fnz + f));
-      bz /= vol;
-      r[2] += bz;
-    }
-  }
-#pragma unroll
-  for (int d = 0; d < NS; ++d) g[d] = r[d];
 }
 
 // correct_interpolation! (Calculate_0_gradient.jl:146-173), internal face f.
@@ -1136,11 +1287,12 @@ __device__ __forceinline__ double midpoint_corrected(const KParams &P, int f) {
 // first interpolation.  With correct_u the last Green-Gauss pass also applies
 // correct_velocity! (Solvers_0_functions.jl:90-99): U = H - grad(p)*rD.
 template <int NS>
-__device__ bool gradient_p(Ctx &C, bool correct_u) {
+__device__ __forceinline__ bool gradient_p(Ctx &C, bool correct_u) {
   const KParams &P = *C.P;
   const int npass = (P.grad == GRAD_MIDPOINT) ? 3 : 1;
   for (int pass = 0; pass < npass; ++pass) {
     const bool last = (pass == npass - 1);
+    C.phase(PH_GRAD);
     tile_each(P, [&](int i) {
       double g[NS];
       green_gauss_row<NS>(P, P.pf, i, g);
@@ -1153,6 +1305,7 @@ __device__ bool gradient_p(Ctx &C, bool correct_u) {
     });
     if (!C.sync()) return false;
     if (!last) {
+      C.phase(PH_FACE);
       grid_each(P.nf - P.nbf, [&](int q) {
         const int f = P.nbf + q;
         P.pf[f] = midpoint_corrected<NS>(P, f);
@@ -1330,10 +1483,11 @@ __device__ __forceinline__ void bound_row(const KParams &P, double *fld, int i) 
 }
 
 template <int NS, typename T>
-__device__ bool turbulence(Ctx &C) {
+__device__ __forceinline__ bool turbulence(Ctx &C) {
   const KParams &P = *C.P;
   const double nu = P.nu;
   // production, destruction, effective diffusivities (turbulence!, :256-272)
+  C.phase(PH_TURB);
   tile_each(P, [&](int i) {
     double g[3][3];
     grad_u_row<NS>(P, i, g);
@@ -1388,6 +1542,7 @@ __device__ bool turbulence(Ctx &C) {
     A.precon = om ? P.precW : P.precK;
     double *phi = om ? P.w : P.k;
     const KCfg &cfg = om ? P.kW : P.kK;
+    C.phase(PH_TURB);
     tile_each(P, [&](int i) {
       double b[1];
       b[0] = om ? scalar_row(P, P.AP, i, phi, P.nueffw, P.Dw, P.Pw, P.bcW, P.aW, P.divW, P.timeW, true)
@@ -1401,6 +1556,7 @@ __device__ bool turbulence(Ctx &C) {
     double rn[1];
     if (!krylov<1, T>(C, A, wk, P.bP, cfg, cfg.solver, its, rn)) return false;
     // run! copy-back, then constrain_boundary! for omega (:401-448)
+    C.phase(PH_TURB);
     tile_each(P, [&](int i) {
       double v = (double)wk.x[i] + phi[i];
       if (om) {
@@ -1425,6 +1581,7 @@ __device__ bool turbulence(Ctx &C) {
   }
   // interpolate!(nutf, nut) + correct_boundaries! + correct_eddy_viscosity! (:496-536)
   // and update_nueff! (Solvers_0_functions.jl:1-11)
+  C.phase(PH_TURB);
   grid_each(P.nf, [&](int f) {
     double v = face_scalar(P, P.nut, f, P.bcN, false);
     if (f < P.nbf) {
@@ -1445,11 +1602,12 @@ __device__ bool turbulence(Ctx &C) {
 
 // ------------------------------------------------------------- programs
 template <int NS, typename T>
-__device__ void simple_program(Ctx &C, int iters, bool piso) {
+__device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
   const KParams &P = *C.P;
   const bool mid = (P.grad == GRAD_MIDPOINT);
   const double nu = P.nu;
   // set-up before the loop (Solvers_1_SIMPLE.jl:114-119)
+  C.phase(PH_SETUP);
   grid_each(P.nf, [&](int f) {
     face_mdot<NS>(P, f);
     P.pf[f] = face_scalar(P, P.p, f, P.bcP, mid);
@@ -1458,6 +1616,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
   });
   if (!C.sync()) return;
   if (!gradient_p<NS>(C, false)) return;
+  C.phase(PH_SETUP);
   int done = 0;
   for (int it = 0; it < iters; ++it) {
     done = it + 1;
@@ -1466,6 +1625,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     // ---- momentum: assemble, start Krylov, set up M, solve
     const MatT<T> &AUT = matU<T>(P);
     const KWorkT<T> &wU = workU<T>(P);
+    C.phase(PH_MOM_ASM);
     tile_each(P, [&](int i) {
       double b[NS];
       momentum_row<NS>(P, i, !piso, b);
@@ -1479,6 +1639,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
 #pragma unroll
     for (int d = 0; d < NS; ++d) finite = finite && isfinite(rnU[d]);
     // run! copy-back: U = x + x0
+    C.phase(PH_UPDATE);
     tile_each(P, [&](int i) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
@@ -1488,6 +1649,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     });
     if (!C.sync()) return;
     // ---- residual!(R_ux..), remove_pressure_source!, H!
+    C.phase(PH_RESID);
     tile_phase<2 * NS>(C, true, [&](int i, double (&v)[2 * NS]) {
       double y[NS], bb[NS];
       spmv_row<NS>(P.AU, i, [&](int j, int d) { return P.U[(size_t)j * NS + d]; }, y);
@@ -1509,7 +1671,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
 #pragma unroll
       for (int d = 0; d < NS; ++d) Rit[d] = sqrt(red[2 * d] / (double)P.n) / sqrt(red[2 * d + 1]);
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (vbid() == 0 && threadIdx.x == 0) {
 #pragma unroll
         for (int d = 0; d < NS; ++d) {
           P.R[(size_t)it * 4 + d] = Rit[d];
@@ -1520,6 +1682,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     const int ncorr = piso ? 2 : 1;
     for (int corr = 0; corr < ncorr; ++corr) {
       if (corr > 0) {   // H! again with the corrected U (PISO corrector loop)
+        C.phase(PH_RESID);
         tile_each(P, [&](int i) {
           double bb[NS];
           ld<NS>(P.bU, i, bb);
@@ -1528,6 +1691,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
         if (!C.sync()) return;
       }
       // interpolate!(rDf, rD); interpolate!(Uf, Hv) + correct_boundaries!
+      C.phase(PH_FACE);
       grid_each(P.nf, [&](int f) {
         const double w = __ldg(P.wgt + f);
         const double omw = 1.0 - w;
@@ -1541,6 +1705,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       // div! + pressure assembly + Krylov start
       const MatT<T> &APT = matP<T>(P);
       const KWorkT<T> &wP = workP<T>(P);
+      C.phase(PH_P_ASM);
       tile_each(P, [&](int i) {
         double b[1];
         b[0] = pressure_row<NS>(P, i);
@@ -1553,6 +1718,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       if (!krylov<1, T>(C, APT, wP, P.bP, P.kP, P.kP.solver, itsP, rnP)) return;
       finite = finite && isfinite(rnP[0]);
       // run! copy-back then explicit_relaxation!(p, prev, alpha_p)
+      C.phase(PH_UPDATE);
       tile_each(P, [&](int i) {
         const double pn = (double)wP.x[i] + P.p[i];
         const double p0 = P.p[i];
@@ -1560,6 +1726,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       });
       if (!C.sync()) return;
       // residual!(R_p) and the face interpolation of grad!(grad p)
+      C.phase(PH_RESID);
       tile_phase<2>(C, true, [&](int i, double (&v)[2]) {
         double y[1];
         spmv_row<1>(P.AP, i, [&](int j, int d) { return P.p[j]; }, y);
@@ -1574,13 +1741,14 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
         double red[2];
         final_sum<2>(P.part, P.ntiles, C.sm, C.sm_out, red);
         Rit[3] = sqrt(red[0] / (double)P.n) / sqrt(red[1]);
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (vbid() == 0 && threadIdx.x == 0) {
           P.R[(size_t)it * 4 + 3] = Rit[3];
           P.kry[(size_t)it * 5 + 3] = itsP[0];
         }
       }
       if (!gradient_p<NS>(C, true)) return;
       // interpolate!(Uf, U) + correct_boundaries! + flux!(mdotf, Uf)
+      C.phase(PH_FACE);
       grid_each(P.nf, [&](int f) { face_mdot<NS>(P, f); });
       if (!C.sync()) return;
       if (P.model == 1 && !turbulence<NS, T>(C)) return;
@@ -1591,7 +1759,7 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
     // Krylov residual norms, which are finite whenever A, b and x0 are.
     if (P.abort_nan) {
       if (!finite) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) P.bar->nonfinite = 1;
+        if (vbid() == 0 && threadIdx.x == 0) P.bar->nonfinite = 1;
         break;
       }
     }
@@ -1606,11 +1774,12 @@ __device__ void simple_program(Ctx &C, int iters, bool piso) {
       if (c) break;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *P.done = done;
+  if (vbid() == 0 && threadIdx.x == 0) *P.done = done;
 }
 
-__device__ void solve_program(Ctx &C) {
+__device__ __forceinline__ void solve_program(Ctx &C) {
   const KParams &P = *C.P;
+  C.phase(PH_P_ASM);
   tile_each(P, [&](int i) {
     double b[1] = {P.sb[i]};
     krylov_init_row<1, double>(P, P.AU, P.AU, P.wU, b, P.U, i, P.solve_solver);
@@ -1626,7 +1795,7 @@ __device__ void solve_program(Ctx &C) {
   double rn[1];
   if (!krylov<1, double>(C, P.AU, P.wU, P.sb, cfg, P.solve_solver, its, rn)) return;
   tile_each(P, [&](int i) { P.U[i] = P.wU.x[i] + P.U[i]; });
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (vbid() == 0 && threadIdx.x == 0) {
     P.solve_out[0] = (double)its[0];
     P.solve_out[1] = rn[0];
     *P.done = 1;
@@ -1648,21 +1817,182 @@ __global__ void __launch_bounds__(TPB, MB) xcal_program_kernel(const __grid_cons
   __shared__ double sm_out[MAXK];
   __shared__ double ws[MAXTL * MAXK * 8];
   __shared__ int sm_ok;
+  __shared__ unsigned long long pacc[2 * NPH];
   Ctx C;
   C.P = &prm;
   C.S.bar = prm.bar;
   C.S.mode = prm.mode;
   C.S.nb = gridDim.x;
+  if (threadIdx.x == 0) {
+    s_vbid = blockIdx.x;
+    s_vnb = gridDim.x;
+  }
+  __syncthreads();
+  C.S.extra = (unsigned)prm.bar_extra;
+  C.S.timeout_ns = prm.bar_timeout_ns ? prm.bar_timeout_ns : BARRIER_TIMEOUT_NS;
   C.S.epoch = 0;
   C.S.ok = &sm_ok;
   C.sm = sm;
   C.sm_out = sm_out;
   C.ws = ws;
+  C.timers = prm.phase != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
+  C.tag = PH_SETUP;
+  C.pacc = pacc;
+  if (C.timers) {
+    for (int k = 0; k < 2 * NPH; ++k) pacc[k] = 0ull;
+    C.t_last = clock64();
+  }
   if (prog == PROG_SOLVE) {
     if constexpr (NS == 1 && sizeof(T) == 8) solve_program(C);
-    return;
+  } else {
+    if constexpr (NS >= 2) simple_program<NS, T>(C, iters, prog == PROG_PISO);
   }
-  if constexpr (NS >= 2) simple_program<NS, T>(C, iters, prog == PROG_PISO);
+  if (C.timers)
+    for (int k = 0; k < 2 * NPH; ++k) prm.phase[k] = pacc[k];
+}
+
+// ------------------------------------------------------------- serving
+// The packed serving form: one persistent launch (all of it co-resident)
+// whose CTAs take cases from the host.  Each CTA polls its mail word in
+// mapped host memory; the host gives a case to a group of CTAs (any CTAs,
+// numbered 0..nblk-1 inside the group), which copy the case's image from
+// pinned host memory into its device region, run SIMPLE to the case's
+// tolerance or iteration cap with a barrier of their own, write the results
+// to pinned host memory and go back to polling.  Every wait is bounded: the
+// group barrier by its 2 s limit, an idle CTA by the host's heartbeat (it
+// leaves when the heartbeat stops for idle_limit_ns, or on shutdown).
+__device__ __forceinline__ unsigned long long ld_acquire_sys_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_sys_i32(int *p, int v) {
+  asm volatile("st.release.sys.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acqrel_u32(unsigned *p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+template <int NS, typename T, int MB>
+__global__ void __launch_bounds__(TPB, MB) xcal_serve_kernel(ServeMail *mail, const ServeCtl *ctl) {
+  __shared__ double sm[8 * MAXK];
+  __shared__ double sm_out[MAXK];
+  __shared__ double ws[MAXTL * MAXK * 8];
+  __shared__ int sm_ok;
+  __shared__ unsigned long long pacc[2 * NPH];
+  __shared__ KParams sP;
+  __shared__ ServeJob *s_job;
+  __shared__ int s_cmd;
+  ServeMail *m = mail + blockIdx.x;
+  unsigned long long seen = 0;
+  if (threadIdx.x == 0) seen = *(volatile unsigned long long *)&m->ack;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int cmd = 0;
+      unsigned long long hb = *(volatile const unsigned long long *)&ctl->heartbeat;
+      unsigned long long t_hb = globaltimer();
+      const unsigned long long limit = ctl->idle_limit_ns;
+      unsigned nap = 256, polls = 0;
+      for (;;) {
+        const unsigned long long q = ld_acquire_sys_u64(&m->seq);
+        if (q != seen) {
+          seen = q;
+          cmd = 1;
+          break;
+        }
+        if ((++polls & 15u) == 0u) {
+          if (*(volatile const unsigned *)&ctl->shutdown) break;
+          const unsigned long long h2 = *(volatile const unsigned long long *)&ctl->heartbeat, now = globaltimer();
+          if (h2 != hb) {
+            hb = h2;
+            t_hb = now;
+          } else if (now - t_hb > limit) {
+            break;
+          }
+        }
+        __nanosleep(nap);
+        if (nap < 32768u) nap <<= 1;
+      }
+      if (cmd) {
+        s_job = m->job;
+        s_vbid = m->vbid;
+        s_vnb = m->nblk;
+        *(volatile unsigned long long *)&m->ack = seen;
+      }
+      s_cmd = cmd;
+    }
+    __syncthreads();
+    if (!s_cmd) return;
+    ServeJob *J = s_job;
+    // the case's parameters into shared memory (read once over the bus)
+    {
+      const unsigned long long *src = (const unsigned long long *)&J->prm;
+      unsigned long long *dst = (unsigned long long *)&sP;
+      for (int k = threadIdx.x; k < (int)(sizeof(KParams) / 8); k += TPB) dst[k] = src[k];
+    }
+    __syncthreads();
+    const int B = vbid(), G = vnb();
+    // this CTA's share of the region: image copy, then zero part
+    {
+      const uint4 *src = J->src;
+      uint4 *dst = J->dst;
+      const unsigned long long c16 = J->copy16, z16 = J->zero16;
+      for (unsigned long long q = (unsigned long long)B * TPB + threadIdx.x; q < c16; q += (unsigned long long)G * TPB)
+        dst[q] = src[q];
+      const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+      for (unsigned long long q = (unsigned long long)B * TPB + threadIdx.x; q < z16; q += (unsigned long long)G * TPB)
+        dst[c16 + q] = zero;
+    }
+    Ctx C;
+    C.P = &sP;
+    C.S.bar = sP.bar;
+    C.S.mode = SYNC_GRID;
+    C.S.nb = G;
+    C.S.extra = 0;
+    C.S.timeout_ns = BARRIER_TIMEOUT_NS;
+    C.S.epoch = 0;
+    C.S.ok = &sm_ok;
+    C.sm = sm;
+    C.sm_out = sm_out;
+    C.ws = ws;
+    C.timers = false;
+    C.tag = PH_SETUP;
+    C.pacc = pacc;
+    C.t_last = 0;
+    if (C.sync()) simple_program<NS, T>(C, J->iters, J->prog == PROG_PISO);
+    C.sync();   // the run's results (fields, histories, done) complete
+    // results to pinned host memory, this CTA's share
+    {
+      const int n = sP.n;
+      const int dn = *(volatile const int *)sP.done;
+      for (int q = B * TPB + threadIdx.x; q < n * NS; q += G * TPB) J->out_U[q] = sP.U[q];
+      for (int q = B * TPB + threadIdx.x; q < n; q += G * TPB) J->out_p[q] = sP.p[q];
+      for (int q = B * TPB + threadIdx.x; q < dn * 4; q += G * TPB) J->out_R[q] = sP.R[q];
+      for (int q = B * TPB + threadIdx.x; q < dn * 5; q += G * TPB) J->out_kry[q] = sP.kry[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence_system();
+      const unsigned prev = atom_add_acqrel_u32(J->exits, 1u);
+      if (prev + 1u == (unsigned)G) {
+        // last CTA of the group out: state for the host, then the group's
+        // barrier word and exit count reset for the next case that uses them
+        volatile Bar *b = sP.bar;
+        J->out_state[0] = *(volatile const int *)sP.done;
+        J->out_state[1] = b->err;
+        J->out_state[2] = b->nonfinite;
+        b->count = 0ull;
+        b->err = 0;
+        b->nonfinite = 0;
+        *(volatile unsigned *)J->exits = 0u;
+        __threadfence_system();
+        st_release_sys_i32(J->out_state + 3, 1);
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // One translation unit per instantiation (build.py compiles this file once per
@@ -1673,10 +2003,17 @@ __global__ void __launch_bounds__(TPB, MB) xcal_program_kernel(const __grid_cons
 #ifndef XCAL_MB
 #define XCAL_MB 2
 #endif
+#if defined(XCAL_SERVE_ONLY)
+template __global__ void xcal_serve_kernel<XCAL_NS, XCAL_T, XCAL_MB>(ServeMail *, const ServeCtl *);
+const void *XCAL_CAT(serve_kernel_, XCAL_INST)() {
+  return (const void *)xcal_serve_kernel<XCAL_NS, XCAL_T, XCAL_MB>;
+}
+#else
 template __global__ void xcal_program_kernel<XCAL_NS, XCAL_T, XCAL_MB>(const __grid_constant__ KParams, int, int);
 const void *XCAL_CAT(program_kernel_, XCAL_INST)() {
   return (const void *)xcal_program_kernel<XCAL_NS, XCAL_T, XCAL_MB>;
 }
+#endif
 #endif
 
 }  // namespace xcal

@@ -13,4 +13,8 @@ int max_coresident_blocks(int ns, int occ, int device);
 int max_cluster_blocks(int ns, int occ = 0);
 const void *program_kernel_ptr(int ns, int mixed, int occ);
 void preload_programs();   // load every build on the current device
+// the serving kernel (xcal_serve_kernel) of a dimension and precision, and the
+// size of its launch on a device
+const void *serve_kernel_ptr(int ns, int mixed);
+int serve_grid(int ns, int mixed, int device);
 }  // namespace xcal

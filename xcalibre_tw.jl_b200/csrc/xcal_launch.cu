@@ -20,6 +20,31 @@ const void *program_kernel_d2o();
 const void *program_kernel_d3o();
 const void *program_kernel_f2o();
 const void *program_kernel_f3o();
+const void *serve_kernel_d2o();
+const void *serve_kernel_d3o();
+const void *serve_kernel_f2o();
+const void *serve_kernel_f3o();
+
+// Serving kernel of a dimension and precision (4-CTA/SM builds).
+const void *serve_kernel_ptr(int ns, int mixed) {
+  if (ns == 2) return mixed ? serve_kernel_f2o() : serve_kernel_d2o();
+  if (ns == 3) return mixed ? serve_kernel_f3o() : serve_kernel_d3o();
+  return nullptr;
+}
+
+// CTAs of the serving launch: every CTA that can be resident at once (a
+// cooperative launch of this size is guaranteed co-resident).
+int serve_grid(int ns, int mixed, int device) {
+  const void *fn = serve_kernel_ptr(ns, mixed);
+  if (!fn) return 0;
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TPB, 0) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sms;
+}
 
 const void *program_kernel_ptr(int ns, int mixed, int occ) {
   if (ns == 1) return program_kernel_d1();

@@ -18,20 +18,40 @@
 
 namespace xcal {
 
-// Per-tile partial sums of (A x - b)^2 and b^2 (one row per thread).
+// Per-tile partial sums of (A x - b)^2 and b^2 (one row per thread).  The
+// CHECKED form (allocation-free entry point, whose CSR arrays are device
+// memory the host cannot validate) reads only inside the CSR's own bounds:
+// a row range outside 0 <= rp[i] <= rp[i+1] <= rp[n] is skipped, as is an
+// entry whose column is outside [0, n); either sets *bad.
+template <bool CHECKED>
 __global__ void __launch_bounds__(TPB) residual_tiles_kernel(int n, const int *__restrict__ rp,
                                                              const int *__restrict__ col,
                                                              const double *__restrict__ val,
                                                              const double *__restrict__ x,
                                                              const double *__restrict__ b, double *part,
-                                                             int ntiles) {
+                                                             int ntiles, int *bad) {
   __shared__ double sm[8 * 2];
   const int t = blockIdx.x;
   const int i = t * TILE + threadIdx.x;
   double v[2] = {0.0, 0.0};
   if (i < n) {
     double y = 0.0;
-    for (int k = rp[i]; k < rp[i + 1]; ++k) y = y + val[k] * x[col[k]];
+    int k0 = rp[i], k1 = rp[i + 1];
+    if (CHECKED) {
+      const int nnz = rp[n];
+      if (k0 < 0 || k1 < k0 || k1 > nnz) {
+        atomicOr(bad, 1);
+        k1 = k0;
+      }
+    }
+    for (int k = k0; k < k1; ++k) {
+      const int j = col[k];
+      if (CHECKED && (j < 0 || j >= n)) {
+        atomicOr(bad, 2);
+        continue;
+      }
+      y = y + val[k] * x[j];
+    }
     const double bi = b[i];
     const double df = y - bi;
     v[0] = df * df;
@@ -53,10 +73,13 @@ __global__ void __launch_bounds__(TPB) residual_final_kernel(int n, const double
 }
 
 cudaError_t launch_residual(int n, const int *rp, const int *col, const double *val, const double *x,
-                            const double *b, double *part, double *out, cudaStream_t stream) {
+                            const double *b, double *part, double *out, cudaStream_t stream, int *bad) {
   const int ntiles = (n + TILE - 1) / TILE;
   (void)cudaGetLastError();   // report this launch's error, not an earlier call's
-  residual_tiles_kernel<<<ntiles, TPB, 0, stream>>>(n, rp, col, val, x, b, part, ntiles);
+  if (bad)
+    residual_tiles_kernel<true><<<ntiles, TPB, 0, stream>>>(n, rp, col, val, x, b, part, ntiles, bad);
+  else
+    residual_tiles_kernel<false><<<ntiles, TPB, 0, stream>>>(n, rp, col, val, x, b, part, ntiles, nullptr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   residual_final_kernel<<<1, TPB, 0, stream>>>(n, part, ntiles, out);
@@ -70,22 +93,31 @@ cudaError_t launch_residual(int n, const int *rp, const int *col, const double *
 constexpr int XCAL_NOALLOC_MAX_TILES = 65536;
 constexpr int XCAL_NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_partials[2 * XCAL_NOALLOC_MAX_TILES];
+// input-check word of the same entry point (bit 1: bad row range, bit 2: bad column)
+static __device__ __align__(256) int g_noalloc_bad;
 
-// Device address of the scratch, resolved once per device with that device
-// current (in host code the symbol names a host-side stand-in, not device memory).
+// Device addresses of the scratch and the check word, resolved once per
+// device with that device current (in host code the symbols name host-side
+// stand-ins, not device memory).  A device reset after the first call on a
+// device is not supported: the cached addresses would be stale.
 static std::mutex g_noalloc_mu;
 static double *g_noalloc_ptr[XCAL_NOALLOC_MAX_DEVICES] = {};
+static int *g_noalloc_bad_ptr[XCAL_NOALLOC_MAX_DEVICES] = {};
 
-cudaError_t noalloc_scratch(int device, double **out) {
+cudaError_t noalloc_scratch(int device, double **out, int **bad) {
   if (device < 0 || device >= XCAL_NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!g_noalloc_ptr[device]) {
-    void *p = nullptr;
+    void *p = nullptr, *q = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess) return e;
+    e = cudaGetSymbolAddress(&q, g_noalloc_bad);
+    if (e != cudaSuccess) return e;
     g_noalloc_ptr[device] = (double *)p;
+    g_noalloc_bad_ptr[device] = (int *)q;
   }
   *out = g_noalloc_ptr[device];
+  *bad = g_noalloc_bad_ptr[device];
   return cudaSuccess;
 }
 

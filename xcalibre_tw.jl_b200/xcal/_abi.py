@@ -31,6 +31,9 @@ RENUMBER_NONE, RENUMBER_RCM, RENUMBER_COLOR = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 FIELD_UX, FIELD_UY, FIELD_UZ, FIELD_P, FIELD_K, FIELD_OMEGA, FIELD_NUT = range(7)
 FLAG_ABORT_ON_NAN, FLAG_PHASE_TIMERS, FLAG_CLUSTER = 1, 2, 4
+# phase classes of the per-phase timers (XCAL_PH_*)
+PHASES = ("setup", "momentum_assembly", "pressure_assembly", "precon_setup", "krylov_spmv",
+          "krylov_precon", "krylov_vector", "residual", "face", "gradient", "update", "turbulence")
 
 P_d = C.POINTER(C.c_double)
 P_i64 = C.POINTER(C.c_int64)
@@ -85,9 +88,28 @@ class Case(C.Structure):
     ]
 
 
+TERM_TIME, TERM_LAPLACIAN, TERM_DIVERGENCE, TERM_SI = 0, 1, 2, 3
+
+
+class Term(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("scheme", C.c_int32), ("sign", C.c_double), ("flux", P_d)]
+
+
+class Source(C.Structure):
+    _fields_ = [("sign", C.c_double), ("field", P_d)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("ctas", C.c_int32), ("ctas_per_sm", C.c_int32), ("cg_fused", C.c_int32),
+                ("candidates", C.c_int32), ("pad", C.c_int32), ("ms_per_iteration", C.c_double),
+                ("ms_default", C.c_double)]
+
+
 class ServeCfg(C.Structure):
     _fields_ = [("slots", C.c_int32), ("max_iterations", C.c_int32), ("renumber", C.c_int32),
-                ("pad", C.c_int32), ("tolerance", C.c_double)]
+                ("precision", C.c_int32), ("tolerance", C.c_double), ("dim", C.c_int32),
+                ("tiles_per_cta", C.c_int32), ("max_ctas", C.c_int32), ("setup_threads", C.c_int32),
+                ("device_bytes", C.c_double), ("host_bytes", C.c_double)]
 
 
 class ServeResult(C.Structure):
@@ -99,7 +121,8 @@ class ServeResult(C.Structure):
 class ServeStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("queued", C.c_int64), ("running", C.c_int64), ("cell_iterations", C.c_double),
-                ("run_ms", C.c_double)]
+                ("run_ms", C.c_double), ("device_bytes", C.c_double), ("device_bytes_peak", C.c_double),
+                ("grid_ctas", C.c_int64)]
 
 
 def dptr(a):
@@ -141,11 +164,18 @@ SIGNATURES = {
     "xcal_simple_run": (C.c_int, [C.c_void_p, C.c_int32, P_d, P_d, P_d, P_d, P_i32, P_i32]),
     "xcal_piso_run": (C.c_int, [C.c_void_p, C.c_int32, P_d, P_d, P_d, P_d, P_i32, P_i32]),
     "xcal_last_run_stats": (C.c_int, [C.c_void_p, P_d, P_d, C.c_int32]),
+    "xcal_last_run_phases": (C.c_int, [C.c_void_p, C.c_int32, P_d, P_i64]),
+    "xcal_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(TuneResult)]),
     "xcal_equation_get": (C.c_int, [C.c_void_p, C.c_int32, P_d, P_d, P_d, P_d]),
     "xcal_linear_solve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int64, P_i32,
                                     P_i32, P_d, P_d, P_d, C.c_int32, C.c_double, C.c_double,
                                     P_i32, P_d]),
     "xcal_residual": (C.c_int, [C.c_void_p, C.c_int64, P_i32, P_i32, P_d, P_d, P_d, P_d]),
+    "xcal_assemble": (C.c_int, [C.c_void_p, C.POINTER(Term), C.c_int32, C.POINTER(Source), C.c_int32,
+                                C.POINTER(BC), C.c_int32, C.c_int32, P_d, P_d, C.c_double, P_d, P_d]),
+    "xcal_spmv": (C.c_int, [C.c_void_p, P_d, P_d, P_d]),
+    "xcal_dilu": (C.c_int, [C.c_void_p, P_d, P_d, P_d]),
+    "xcal_grad": (C.c_int, [C.c_void_p, P_d, C.POINTER(BC), C.c_int32, P_d]),
     "xcal_residual_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_void_p]),
     "xcal_ctx_set_tolerance": (C.c_int, [C.c_void_p, C.c_double]),

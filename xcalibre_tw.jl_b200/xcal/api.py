@@ -443,6 +443,23 @@ class Solver:
         self.lib.xcal_last_run_stats(self.ctx, _abi.dptr(ms), None, 0)
         return float(ms[0])
 
+    def autotune(self, iterations=3):
+        """xcal_autotune: time the launch forms on this case (fields restored),
+        keep the fastest; returns the choice as a dict."""
+        r = _abi.TuneResult()
+        _abi.check(self.lib.xcal_autotune(self.ctx, int(iterations), C.byref(r)), self.ctx, "xcal_autotune")
+        return {k: getattr(r, k) for k, _ in _abi.TuneResult._fields_ if k != "pad"}
+
+    def last_phases(self):
+        """Per-phase-class SM cycles and phase counts of the last run (context
+        created with FLAG_PHASE_TIMERS): {class: (cycles, count)}."""
+        n = len(_abi.PHASES)
+        cyc = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int64)
+        _abi.check(self.lib.xcal_last_run_phases(self.ctx, n, _abi.dptr(cyc), _abi.i64ptr(cnt)), self.ctx,
+                   "xcal_last_run_phases")
+        return {k: (float(cyc[i]), int(cnt[i])) for i, k in enumerate(_abi.PHASES)}
+
     def equation(self, which):
         n = self.n
         nnz = n + int(self.mesh.cell_faces_ptr[-1] - 1)
@@ -542,27 +559,36 @@ def model2vtk(model, name):
 
 
 class Server:
-    """A stream of independent cases on one GPU (xcal_serve_*): `slots` worker
-    threads, each running its cases as one hardware cluster on its own stream,
-    every case until all residuals are <= tolerance or max_iterations.
-    slots <= 30 keeps one hardware work queue per worker with the 32 queues
-    the package asks the driver for on import (CUDA_DEVICE_MAX_CONNECTIONS)."""
+    """A stream of independent cases on one GPU (xcal_serve_*): one persistent
+    launch for the server's lifetime; each case is admitted when its device
+    footprint fits the server's arena, laid out by host set-up threads and
+    run to `tolerance` or `max_iterations` by a group of the launch's CTAs
+    sized by its mesh, beside the other cases in flight.  Every case has the
+    mesh dimension `dim` and runs in `precision`.  While a server exists it
+    holds the GPU: other device work of the process waits until close()."""
 
-    def __init__(self, device=0, slots=16, max_iterations=3000, tolerance=1e-6,
-                 renumber=_abi.RENUMBER_COLOR):
+    def __init__(self, device=0, slots=256, max_iterations=3000, tolerance=1e-6,
+                 renumber=_abi.RENUMBER_COLOR, precision=_abi.PREC_MIXED, dim=2, tiles_per_cta=0,
+                 max_ctas=0, setup_threads=0, device_bytes=0.0, host_bytes=0.0):
         self.lib = _abi.load()
-        cfg = _abi.ServeCfg(slots=slots, max_iterations=max_iterations, renumber=renumber, pad=0,
-                            tolerance=tolerance)
+        self.precision = precision
+        cfg = _abi.ServeCfg(slots=slots, max_iterations=max_iterations, renumber=renumber, precision=precision,
+                            tolerance=tolerance, dim=dim, tiles_per_cta=tiles_per_cta, max_ctas=max_ctas,
+                            setup_threads=setup_threads, device_bytes=float(device_bytes),
+                            host_bytes=float(host_bytes))
         h = C.c_void_p()
         _abi.check(self.lib.xcal_serve_create(device, C.byref(cfg), C.byref(h)), None, "xcal_serve_create")
         self.srv = h
         self.ncells = {}
 
-    def submit(self, model, config, pref=None, precision=_abi.PREC_MIXED):
+    def submit(self, model, config, pref=None, precision=None):
         """Queue simple!(model, config; pref) with the model's current fields as
-        the initial condition; returns a ticket."""
+        the initial condition; returns a ticket.  The case runs in the
+        server's precision (a different `precision` raises)."""
+        if precision is not None and precision != self.precision:
+            raise _abi.XcalError("xcal_serve_submit: the server runs every case in its own precision")
         mesh = model.mesh
-        case, keep = make_case(model, config, pref, precision)
+        case, keep = make_case(model, config, pref, self.precision)
         n = mesh.ncells
         U = np.ascontiguousarray(np.stack([model.U.x.values, model.U.y.values, model.U.z.values]).reshape(3 * n),
                                  dtype=np.float64)

@@ -96,13 +96,13 @@ def fields(model):
     return U.reshape(3, n).copy(), model.p.values.copy()
 
 
-def flatplate(nx=600, ny=250, iterations=3000, wall_functions=False, **kw):
+def flatplate(nx=600, ny=250, iterations=3000, wall_functions=False, mesh=None, **kw):
     """k-omega flat plate 1 m x 0.2 m, U = 10 m/s, nu = 1.5e-5, inlet k from 1 %
     intensity (0.015) and omega from a viscosity ratio of 10 (100); BCs as the
     reference's low-Re flat-plate case (omega wall function on the plate).  With
     wall_functions, k and nut also use their wall functions on the plate."""
-    path = _unv("flatplate", meshgen.flatplate_unv, nx=nx, ny=ny)
-    mesh = X.build_mesh(path)
+    if mesh is None:
+        mesh = X.build_mesh(_unv("flatplate", meshgen.flatplate_unv, nx=nx, ny=ny))
     model = X.RANS(X.KOmega, mesh=mesh, viscosity=X.ConstantScalar(1.5e-5))
     Uin, kin = 10.0, 1.5 * (0.01 * 10.0) ** 2
     win = kin / (10 * 1.5e-5)
