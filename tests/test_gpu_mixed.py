@@ -8,15 +8,11 @@ the difference:
   of the FP64 oracle's converged fields, the iteration count within 5 %;
 * 30 iterations of the 3D cavity (every Krylov solve reaches its tolerance):
   fields within 1e-4 relative L2 of the oracle;
-* the BFS, whose pressure CG stops at itmax = 100 before its tolerance for
-  hundreds of SIMPLE iterations: its early trajectory is not comparable (an
-  unconverged 100-step CG amplifies rounding differences), so both precisions
-  are run to convergence (about 790 iterations) and compared there, the FP64
-  side being the device's FP64 run (bitwise equal to the oracle on this case,
-  see test_gpu_parity.py): fields within 2e-4 relative L2 and the iteration
-  counts within 2 %.  Two converged SIMPLE runs that stop at the 1e-7 residual
-  criterion at slightly different points differ by about the residual divided
-  by the per-iteration contraction gap (0.98 here), which is this order.
+  (an unconverged trajectory, where the 1e-6 contract does not apply).
+
+The converged BFS and hex cavity, compared at a fixed iteration count far
+past the stop test, and the 128^3 cavity at its 500 iterations are held to
+1e-6 in test_gpu_configs.py.
 """
 import pytest
 
@@ -27,7 +23,6 @@ pytestmark = pytest.mark.gpu
 
 CONVERGED_TOL = 1e-6
 TRAJECTORY_TOL = 1e-4
-BFS_CONVERGED_TOL = 2e-4
 
 
 def test_mixed_cavity_converged():
@@ -52,15 +47,3 @@ def test_mixed_hex_trajectory():
     for k in ("U0", "U1", "U2", "p"):
         assert d[k] <= TRAJECTORY_TOL, (k, d[k])
 
-
-def test_mixed_bfs_converged():
-    its = 1500
-    mesh, model, config, pref = cases.bfs(27, iterations=its)
-    d64 = run_device(mesh, model, config, pref, its, _abi.RENUMBER_COLOR)
-    d32 = run_device(mesh, model, config, pref, its, _abi.RENUMBER_COLOR, precision=_abi.PREC_MIXED)
-    assert d64["done"] < its and d32["done"] < its, "both precisions converge below 1e-7"
-    assert abs(d32["done"] - d64["done"]) <= 0.02 * d64["done"], (d32["done"], d64["done"])
-    d = compare(d32, d64, 2, check_eqns=False)
-    print("mixed bfs", d32["done"], d64["done"], d)
-    for k in ("U0", "U1", "p"):
-        assert d[k] <= BFS_CONVERGED_TOL, (k, d[k])

@@ -66,6 +66,28 @@ def test_serve_matches_alone(precision):
             assert d <= 1e-3
 
 
+
+def test_serve_concurrent_groups_repeatable():
+    """Several multi-CTA cases in flight at once, repeated: every result equals
+    the case run alone, bit for bit, in every repetition.  Groups of
+    different cases share SMs, so a group's CTAs run at uneven speeds; a CTA
+    that is still reading one reduction's partial sums while a faster CTA of
+    its group writes the next reduction's must not see the new values (the
+    partial sums are double-buffered for this)."""
+    stream = cases.serving_stream(6, rate=1000.0, seed=7, nmin=16, nmax=48, re_max=60.0)
+    alone = [_alone(c, _abi.PREC_FP64) for c in stream]
+    for rep in range(3):
+        srv = X.Server(slots=4, max_iterations=MAXIT, tolerance=TOL, precision=_abi.PREC_FP64, tiles_per_cta=1)
+        try:
+            tickets = [srv.submit(c["model"], c["config"], c["pref"]) for c in stream]
+            results = [srv.poll(t, wait_ms=-1) for t in tickets]
+        finally:
+            srv.close()
+        for k, (r, a) in enumerate(zip(results, alone)):
+            assert r["status"] == 0, (rep, k, r["status"])
+            assert r["iterations"] == a["done"], (rep, k, r["iterations"], a["done"])
+            assert np.array_equal(r["U"], a["U"]) and np.array_equal(r["p"], a["p"]), (rep, k)
+
 def test_serve_stats_and_errors():
     srv = X.Server(slots=2, max_iterations=50, tolerance=TOL)
     try:

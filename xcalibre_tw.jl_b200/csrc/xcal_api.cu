@@ -769,7 +769,7 @@ static int case_arrays(xcal_ctx c, const xcal_case *cfg, Sink &B, const double *
     w->x = A(m); w->s = A(m); w->t = A(m); w->q = A(m);
     for (int b = 0; b < 2; ++b) { w->r[b] = A(m); w->p[b] = A(m); w->v[b] = A(m); }
   }
-  h.part = A((size_t)MAXK * h.ntiles);
+  h.part = A((size_t)2 * MAXK * h.ntiles);   // two buffers, used in turn
   // ILU(0) factors and GMRES work space where a solver asks for them (k and
   // omega reuse the pressure matrix and work set)
   auto is_ilu = [](const xcal_solver_cfg &sc) { return sc.preconditioner == XCAL_PRECON_ILU0; };
@@ -792,7 +792,7 @@ static int case_arrays(xcal_ctx c, const xcal_case *cfg, Sink &B, const double *
       const Mat &M64 = (k == 0) ? h.AU : h.AP;
       M32.col = M64.col; M32.tpos = M64.tpos; M32.dpos = M64.dpos; M32.W = M64.W; M32.np = M64.np;
       M32.precon = M64.precon;
-      M32.val = F(nnz); M32.Dpiv = F(n); M32.Dinv = F(n);
+      M32.val = B.zeros_n<float>(nnz); M32.Dpiv = F(n); M32.Dinv = F(n);   // padding zero, as in FP64
       M32.fval = M64.fval ? F(nnz) : nullptr;
       KWorkT<float> *w = (k == 0) ? &h.wU32 : &h.wP32;
       size_t m = (k == 0) ? (size_t)n * NS : (size_t)n;
@@ -1273,7 +1273,7 @@ int xcal_linear_solve(xcal_ctx c, int32_t solver, int32_t precon, int64_t n64, c
   KWork &w = h.wU;
   w.x = A(n); w.s = A(n); w.t = A(n); w.q = A(n);
   for (int k = 0; k < 2; ++k) { w.r[k] = A(n); w.p[k] = A(n); w.v[k] = A(n); }
-  h.part = A((size_t)MAXK * h.ntiles);
+  h.part = A((size_t)2 * MAXK * h.ntiles);   // two buffers, used in turn
   h.solve_out = A(2);
   h.bar = B.alloc<Bar>(1);
   h.done = B.alloc<int>(1);

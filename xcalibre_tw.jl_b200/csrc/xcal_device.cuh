@@ -189,6 +189,25 @@ struct ServeCtl {
 };
 
 // ------------------------------------------------------------------ helpers
+// Loads of arrays that do not change while a case runs (geometry, matrix
+// pattern, level sets, boundary tables).  An ordinary launch uploads them
+// before it starts, so they go through the read-only data path
+// (ld.global.nc).  The serving kernel writes each case's arrays into its
+// arena itself and reuses arena memory for later cases within the same
+// launch: for it the arrays are not read-only for the kernel's lifetime, so
+// its build (XCAL_SERVE_ONLY) reads them with ordinary coherent loads.
+#if defined(XCAL_SERVE_ONLY)
+template <class V>
+__device__ __forceinline__ V ldro(const V *p) {
+  return *p;
+}
+#else
+template <class V>
+__device__ __forceinline__ V ldro(const V *p) {
+  return __ldg(p);
+}
+#endif
+
 __device__ __forceinline__ double jmax(double a, double b) {
   if (a != a || b != b) return a + b;
   if (a > b) return a;
@@ -347,7 +366,7 @@ struct Row {
 template <typename T>
 __device__ __forceinline__ void load_row(const MatT<T> &A, int i, Row &r) {
 #pragma unroll
-  for (int k = 0; k < WUNROLL; ++k) r.c[k] = (k < A.W) ? __ldg(A.col + (size_t)k * A.np + i) : -1;
+  for (int k = 0; k < WUNROLL; ++k) r.c[k] = (k < A.W) ? ldro(A.col + (size_t)k * A.np + i) : -1;
 }
 
 // Row routines keep their loads out of data-dependent branches: a padding
@@ -382,7 +401,7 @@ __device__ __forceinline__ void spmv_row(const MatT<T> &A, int i, GetX getx, T (
     }
   } else {
     for (int k = 0; k < A.W; ++k) {
-      const int j = __ldg(A.col + (size_t)k * A.np + i);
+      const int j = ldro(A.col + (size_t)k * A.np + i);
       if (j < 0) continue;
       const T a = A.val[(size_t)k * A.np + i];
 #pragma unroll
@@ -395,7 +414,7 @@ __device__ __forceinline__ void spmv_row(const MatT<T> &A, int i, GetX getx, T (
 // D_i = A_ii - sum_{j<i} (A_ij*A_ji)/D_j over lower neighbours in ascending j.
 template <typename T>
 __device__ __forceinline__ void dilu_setup_row(const MatT<T> &A, int i) {
-  T D = A.val[__ldg(A.dpos + i)];
+  T D = A.val[ldro(A.dpos + i)];
   if (A.W <= WUNROLL) {
     // Row entries are in ascending column order, so the lower neighbours are
     // the entries with 0 <= j < i.
@@ -407,7 +426,7 @@ __device__ __forceinline__ void dilu_setup_row(const MatT<T> &A, int i) {
       const size_t e = (size_t)kk * A.np + i;
       const int c = r.c[k];
       const bool use = c >= 0 && c < i;
-      const int tp = __ldg(A.tpos + e);
+      const int tp = ldro(A.tpos + e);
       const int j = use ? c : i;
       const T t = D - A.val[e] * A.val[use ? tp : (int)e] / A.Dpiv[j];
       D = use ? t : D;
@@ -415,9 +434,9 @@ __device__ __forceinline__ void dilu_setup_row(const MatT<T> &A, int i) {
   } else {
     for (int k = 0; k < A.W; ++k) {
       const size_t e = (size_t)k * A.np + i;
-      const int j = __ldg(A.col + e);
+      const int j = ldro(A.col + e);
       if (j < 0 || j >= i) break;
-      D = D - A.val[e] * A.val[__ldg(A.tpos + e)] / A.Dpiv[j];
+      D = D - A.val[e] * A.val[ldro(A.tpos + e)] / A.Dpiv[j];
     }
   }
   A.Dpiv[i] = D;
@@ -451,7 +470,7 @@ __device__ __forceinline__ void dilu_fwd_row(const MatT<T> &A, const T (&in)[NS]
   } else {
     for (int k = 0; k < A.W; ++k) {
       const size_t e = (size_t)k * A.np + i;
-      const int j = __ldg(A.col + e);
+      const int j = ldro(A.col + e);
       if (j < 0 || j >= i) break;
       const T a = A.val[e], dj = A.Dinv[j];
 #pragma unroll
@@ -492,7 +511,7 @@ __device__ __forceinline__ void dilu_bwd_row_g(const MatT<T> &A, const T (&out_i
   } else {
     for (int k = 0; k < A.W; ++k) {
       const size_t e = (size_t)k * A.np + i;
-      const int j = __ldg(A.col + e);
+      const int j = ldro(A.col + e);
       if (j <= i) continue;
       const T a = A.val[e];
 #pragma unroll
@@ -633,7 +652,7 @@ __device__ __forceinline__ void dilu_bwd_row(const MatT<T> &A, const T *out, int
 template <typename T>
 __device__ __forceinline__ T ell_find(const MatT<T> &A, const T *vals, int row, int colj) {
   for (int k = 0; k < A.W; ++k) {
-    const int c = __ldg(A.col + (size_t)k * A.np + row);
+    const int c = ldro(A.col + (size_t)k * A.np + row);
     if (c == colj) return vals[(size_t)k * A.np + row];
     if (c < 0 || c > colj) break;
   }
@@ -642,7 +661,7 @@ __device__ __forceinline__ T ell_find(const MatT<T> &A, const T *vals, int row, 
 template <typename T>
 __device__ __forceinline__ bool ell_has(const MatT<T> &A, int row, int colj) {
   for (int k = 0; k < A.W; ++k) {
-    const int c = __ldg(A.col + (size_t)k * A.np + row);
+    const int c = ldro(A.col + (size_t)k * A.np + row);
     if (c == colj) return true;
     if (c < 0 || c > colj) break;
   }
@@ -657,14 +676,14 @@ __device__ __forceinline__ void ilu_setup_row(const MatT<T> &A, int i) {
   }
   for (int k = 0; k < A.W; ++k) {
     const size_t e = (size_t)k * A.np + i;
-    const int kk = __ldg(A.col + e);
+    const int kk = ldro(A.col + e);
     if (kk < 0 || kk >= i) break;
-    const T ukk = A.fval[__ldg(A.dpos + kk)];
+    const T ukk = A.fval[ldro(A.dpos + kk)];
     const T l = A.fval[e] * (T(1) / ukk);
     A.fval[e] = l;
     for (int m = k + 1; m < A.W; ++m) {
       const size_t em = (size_t)m * A.np + i;
-      const int j = __ldg(A.col + em);
+      const int j = ldro(A.col + em);
       if (j < 0) break;
       if (ell_has(A, kk, j)) A.fval[em] = A.fval[em] - l * ell_find(A, (const T *)A.fval, kk, j);
     }
@@ -678,14 +697,14 @@ __device__ __forceinline__ void ilu_fwd_row(const MatT<T> &A, const T (&in)[NS],
   for (int d = 0; d < NS; ++d) o[d] = in[d];
   for (int k = 0; k < A.W; ++k) {
     const size_t e = (size_t)k * A.np + i;
-    const int j = __ldg(A.col + e);
+    const int j = ldro(A.col + e);
     if (j < 0 || j >= i) break;
     const T l = A.fval[e];
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = o[d] - l * geto(j, d);
   }
   if (blev_i == 0) {
-    const T u = A.fval[__ldg(A.dpos + i)];
+    const T u = A.fval[ldro(A.dpos + i)];
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = o[d] / u;
   }
@@ -698,13 +717,13 @@ __device__ __forceinline__ void ilu_bwd_row_g(const MatT<T> &A, const T (&out_i)
   for (int d = 0; d < NS; ++d) o[d] = out_i[d];
   for (int k = A.W - 1; k >= 0; --k) {
     const size_t e = (size_t)k * A.np + i;
-    const int j = __ldg(A.col + e);
+    const int j = ldro(A.col + e);
     if (j <= i) continue;
     const T u = A.fval[e];
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = o[d] - u * geto(j, d);
   }
-  const T u = A.fval[__ldg(A.dpos + i)];
+  const T u = A.fval[ldro(A.dpos + i)];
 #pragma unroll
   for (int d = 0; d < NS; ++d) o[d] = o[d] / u;
 }
@@ -714,13 +733,13 @@ __device__ __forceinline__ void ilu_bwd_row_g(const MatT<T> &A, const T (&out_i)
 template <typename T>
 __device__ __forceinline__ void diag_precon_setup_row(const MatT<T> &A, int i) {
   if (A.precon == 1) {
-    A.Dinv[i] = T(1) / fabs(A.val[__ldg(A.dpos + i)]);
+    A.Dinv[i] = T(1) / fabs(A.val[ldro(A.dpos + i)]);
   } else if (A.precon == 2) {
     T s = T(0);
     for (int k = 0; k < A.W; ++k) {
       const size_t e = (size_t)k * A.np + i;
-      if (__ldg(A.col + e) < 0) continue;
-      const T a = A.val[__ldg(A.tpos + e)];
+      if (ldro(A.col + e) < 0) continue;
+      const T a = A.val[ldro(A.tpos + e)];
       s += a * a;
     }
     A.Dinv[i] = T(1) / sqrt(s);
@@ -734,17 +753,17 @@ __device__ __forceinline__ void diag_precon_setup_row(const MatT<T> &A, int i) {
 // (:6-110) of a scalar cell field at face f.
 __device__ __forceinline__ double face_scalar(const KParams &P, const double *cellv, int f, const FieldBC &bc,
                                               bool midpoint) {
-  const int a = __ldg(P.o1 + f), b = __ldg(P.o2 + f);
+  const int a = ldro(P.o1 + f), b = ldro(P.o2 + f);
   double v;
   if (midpoint) {
     v = 0.5 * (cellv[a] + cellv[b]);
   } else {
-    const double w = __ldg(P.wgt + f);
+    const double w = ldro(P.wgt + f);
     const double omw = 1.0 - w;
     v = w * cellv[a] + omw * cellv[b];
   }
   if (f < P.nbf) {
-    const int bi = __ldg(bc.fbc + f);
+    const int bi = ldro(bc.fbc + f);
     if (bi >= 0) {
       const BcEntry &e = bc.tab[bi];
       v = (e.type == BC_DIRICHLET) ? e.v[0] : cellv[a];
@@ -759,27 +778,27 @@ __device__ __forceinline__ void green_gauss_row(const KParams &P, const double *
   double r[3] = {0.0, 0.0, 0.0};
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
+    const int f = ldro(P.f_face + e);
     if (f < 0) break;
-    const double ns = (double)__ldg(P.f_sign + e);
-    const double a = __ldg(P.area + f), v = pf[f];
-    r[0] += v * ((a * __ldg(P.fnx + f)) * ns);
-    r[1] += v * ((a * __ldg(P.fny + f)) * ns);
-    if (NS == 3) r[2] += v * ((a * __ldg(P.fnz + f)) * ns);
+    const double ns = (double)ldro(P.f_sign + e);
+    const double a = ldro(P.area + f), v = pf[f];
+    r[0] += v * ((a * ldro(P.fnx + f)) * ns);
+    r[1] += v * ((a * ldro(P.fny + f)) * ns);
+    if (NS == 3) r[2] += v * ((a * ldro(P.fnz + f)) * ns);
   }
-  const double vol = __ldg(P.vol + i);
+  const double vol = ldro(P.vol + i);
 #pragma unroll
   for (int d = 0; d < NS; ++d) r[d] /= vol;
-  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q) {
-    const int f = __ldg(P.cb_face + q);
-    const double a = __ldg(P.area + f), v = pf[f];
-    double bx = v * (a * __ldg(P.fnx + f)), by = v * (a * __ldg(P.fny + f));
+  for (int q = ldro(P.cb_ptr + i); q < ldro(P.cb_ptr + i + 1); ++q) {
+    const int f = ldro(P.cb_face + q);
+    const double a = ldro(P.area + f), v = pf[f];
+    double bx = v * (a * ldro(P.fnx + f)), by = v * (a * ldro(P.fny + f));
     bx /= vol;
     by /= vol;
     r[0] += bx;
     r[1] += by;
     if (NS == 3) {
-      double bz = v * (a * __ldg(P.fnz + f));
+      double bz = v * (a * ldro(P.fnz + f));
       bz /= vol;
       r[2] += bz;
     }

@@ -52,6 +52,16 @@ constexpr int MAXTL = 32;   // tiles per CTA whose warp sums are staged in share
 struct Ctx {
   const KParams *P;
   Sync S;
+  // Per-tile partial sums, two buffers of MAXK*ntiles used in turn by
+  // successive reducing phases.  A CTA reads a reduction's partials after the
+  // barrier that ends its phase while faster CTAs may already be writing the
+  // next reduction's partials; with a single buffer that write could land
+  // before the read.  The next write to the same buffer comes two reducing
+  // phases later, behind a barrier every CTA reaches only after its read.
+  double *part;
+  int pw;   // buffer the next reducing phase writes
+  __device__ __forceinline__ double *part_w() const { return part + (size_t)pw * MAXK * P->ntiles; }
+  __device__ __forceinline__ const double *part_r() const { return part + (size_t)(pw ^ 1) * MAXK * P->ntiles; }
   double *sm;       // [8*MAXK]
   double *sm_out;   // [MAXK]
   double *ws;       // [MAXTL*MAXK*8] staged warp sums
@@ -101,7 +111,8 @@ __device__ __forceinline__ void tile_each(const KParams &P, F f) {
 }
 
 // One row per thread per tile; with `reduce`, the K values returned by f are
-// summed per tile with the canonical tree into part[k*ntiles + t].  The warp
+// summed per tile with the canonical tree into part[k*ntiles + t] of the
+// current partial-sum buffer (Ctx::part_w).  The warp
 // stage of each tile's tree runs as the rows finish and is staged in shared
 // memory; the 8-way stage of all the CTA's tiles runs once at the end, so the
 // warps are not held at a block barrier per tile.
@@ -118,6 +129,8 @@ __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
     return;
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double *part = C.part_w();
+  C.pw ^= 1;
   for (int t0 = B; t0 < nt; t0 += MAXTL * G) {   // chunks of at most MAXTL tiles
     int tl = 0;
     for (int t = t0; t < nt && tl < MAXTL; t += G, ++tl) {
@@ -142,7 +155,7 @@ __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
       a1 = a1 + a3;
       a0 = a0 + a1;
       const int k = q % K, t = t0 + (q / K) * G;
-      P.part[(size_t)k * nt + t] = a0;
+      part[(size_t)k * nt + t] = a0;
     }
     __syncthreads();
   }
@@ -166,6 +179,8 @@ __device__ __forceinline__ void tile_phase_rows(Ctx &C, bool reduce, F f) {
   const KParams &P = *C.P;
   const int G = vnb(), nt = P.ntiles, B = vbid();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double *part = C.part_w();
+  if (reduce) C.pw ^= 1;
   for (int t0 = B; t0 < nt; t0 += MAXTL * G) {
     int tl = 0;
     for (int t = t0; t < nt && tl < MAXTL; t += R * G, tl += R) {
@@ -209,7 +224,7 @@ __device__ __forceinline__ void tile_phase_rows(Ctx &C, bool reduce, F f) {
       a1 = a1 + a3;
       a0 = a0 + a1;
       const int k = q % K, t = t0 + (q / K) * G;
-      P.part[(size_t)k * nt + t] = a0;
+      part[(size_t)k * nt + t] = a0;
     }
     __syncthreads();
   }
@@ -239,10 +254,10 @@ template <int NS, typename T>
 __device__ __forceinline__ bool precon_local(const KParams &P, const MatT<T> &A, int i, const T (&in)[NS],
                                              T (&o)[NS]) {
   if (A.precon == PRECON_DILU) {
-    if (__ldg(P.flev + i) != 0) return false;
+    if (ldro(P.flev + i) != 0) return false;
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = in[d];
-    if (__ldg(P.blev + i) == 0) {
+    if (ldro(P.blev + i) == 0) {
       const T di = A.Dinv[i];
 #pragma unroll
       for (int d = 0; d < NS; ++d) o[d] = o[d] * di;
@@ -250,11 +265,11 @@ __device__ __forceinline__ bool precon_local(const KParams &P, const MatT<T> &A,
     return true;
   }
   if (A.precon == PRECON_ILU0) {
-    if (__ldg(P.flev + i) != 0) return false;
+    if (ldro(P.flev + i) != 0) return false;
 #pragma unroll
     for (int d = 0; d < NS; ++d) o[d] = in[d];
-    if (__ldg(P.blev + i) == 0) {
-      const T u = A.fval[__ldg(A.dpos + i)];
+    if (ldro(P.blev + i) == 0) {
+      const T u = A.fval[ldro(A.dpos + i)];
 #pragma unroll
       for (int d = 0; d < NS; ++d) o[d] = o[d] / u;
     }
@@ -294,14 +309,14 @@ __device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *i
           int bl[R];
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            bl[r] = __ldg(P.blev + ii[r]);
+            bl[r] = ldro(P.blev + ii[r]);
 #pragma unroll
             for (int d = 0; d < NS; ++d) iv[r][d] = in[(size_t)ii[r] * NS + d];
           }
           dilu_fwd_rows<R, NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, ii, bl, o);
 #pragma unroll
           for (int r = 0; r < R; ++r)
-            if (ok[r] && __ldg(P.flev + ii[r]) == l)
+            if (ok[r] && ldro(P.flev + ii[r]) == l)
 #pragma unroll
               for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
           if (last)
@@ -318,7 +333,7 @@ __device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *i
           dilu_bwd_rows<R, NS>(A, out, ii, o);
 #pragma unroll
           for (int r = 0; r < R; ++r)
-            if (ok[r] && __ldg(P.blev + ii[r]) == l)
+            if (ok[r] && ldro(P.blev + ii[r]) == l)
 #pragma unroll
               for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
           if (last)
@@ -350,12 +365,12 @@ __device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *i
   for (int l = first_lvl; l < P.nfl; ++l) {
     const bool last = (++ph == nph);
     tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
-      if (__ldg(P.flev + i) == l) {
+      if (ldro(P.flev + i) == l) {
         if (setup) lev_setup_row(A, i);
         T iv[NS], o[NS];
 #pragma unroll
         for (int d = 0; d < NS; ++d) iv[d] = in[(size_t)i * NS + d];
-        lev_fwd_row<NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, __ldg(P.blev + i), o);
+        lev_fwd_row<NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, i, ldro(P.blev + i), o);
 #pragma unroll
         for (int d = 0; d < NS; ++d) out[(size_t)i * NS + d] = o[d];
       }
@@ -366,7 +381,7 @@ __device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *i
   for (int l = 1; l < P.nbl; ++l) {
     const bool last = (++ph == nph);
     tile_phase<K>(C, last, [&](int i, double (&v)[K]) {
-      if (__ldg(P.blev + i) == l) {
+      if (ldro(P.blev + i) == l) {
         T o[NS];
         lev_bwd_row<NS>(A, out, i, o);
 #pragma unroll
@@ -391,9 +406,10 @@ __device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A64
                                                 const KWorkT<T> &w, const double (&b)[NS], const double *x0,
                                                 int i, int solver) {
   if constexpr (sizeof(T) == 4) {
+    // every entry, padding included (zero in the FP64 matrix)
     for (int k = 0; k < A.W; ++k) {
       const size_t e = (size_t)k * A.np + i;
-      if (__ldg(A.col + e) >= 0) A.val[e] = (float)A64.val[e];
+      A.val[e] = (float)A64.val[e];
     }
   }
   double y[NS];
@@ -404,7 +420,7 @@ __device__ __forceinline__ void krylov_init_row(const KParams &P, const Mat &A64
     r0[d] = (T)(b[d] - y[d]);
     w.x[(size_t)i * NS + d] = T(0);
   }
-  if (leveled(A) && __ldg(P.flev + i) == 0) lev_setup_row(A, i);
+  if (leveled(A) && ldro(P.flev + i) == 0) lev_setup_row(A, i);
   T o[NS];
   const bool dilu = leveled(A);
   if (solver != SOLVER_CG) {
@@ -459,7 +475,7 @@ __device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<
                          int (&its)[NS], double (&rnorm_out)[NS]) {
   const KParams &P = *C.P;
   double red[2 * NS];
-  final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+  final_sum<2 * NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
   double rho[NS], alpha[NS], omega[NS], beta[NS], rnorm[NS], eps[NS], nrho[NS];
   unsigned active = 0;
 #pragma unroll
@@ -517,7 +533,7 @@ __device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<
       return false;
     {
       double cv[NS];
-      final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, cv);
+      final_sum<NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, cv);
 #pragma unroll
       for (int d = 0; d < NS; ++d)
         if (active & (1u << d)) alpha[d] = rho[d] / cv[d];
@@ -563,7 +579,7 @@ __device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<
           }
         }))
       return false;
-    final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+    final_sum<2 * NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
 #pragma unroll
     for (int d = 0; d < NS; ++d)
       if (active & (1u << d)) omega[d] = red[2 * d] / red[2 * d + 1];
@@ -586,7 +602,7 @@ __device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<
       }
     });
     if (!C.sync()) return false;
-    final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+    final_sum<2 * NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
     unsigned cont = 0;
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
@@ -625,7 +641,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
   const KParams &P = *C.P;
   const double EPS = 2.220446049250313e-16;
   double red[NS];
-  final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+  final_sum<NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
   double gamma[NS], sgn[NS], rnorm[NS], pn2[NS], eps[NS], alpha[NS], beta[NS];
   unsigned active = 0;
 #pragma unroll
@@ -694,7 +710,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
       });
     }
     if (!C.sync()) return false;
-    final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+    final_sum<NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
     unsigned upd = 0;
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
@@ -725,8 +741,8 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const int i = ii[r];
-            fl[r] = __ldg(P.flev + i);
-            bl[r] = __ldg(P.blev + i);
+            fl[r] = ldro(P.flev + i);
+            bl[r] = ldro(P.blev + i);
 #pragma unroll
             for (int d = 0; d < NS; ++d) {
               const size_t k = (size_t)i * NS + d;
@@ -766,9 +782,9 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
       }
       bool have;
       if (fuse) {
-        if (__ldg(P.flev + i) == 1) {
+        if (ldro(P.flev + i) == 1) {
           dilu_fwd_row<NS>(A, rr, getr, i, 0, o);
-        } else if (__ldg(P.blev + i) == 0) {
+        } else if (ldro(P.blev + i) == 0) {
 #pragma unroll
           for (int d = 0; d < NS; ++d) o[d] = rr[d] * A.Dinv[i];
         } else {
@@ -783,8 +799,8 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
         have = true;
       } else {
         have = precon_local<NS>(P, A, i, rr, o);
-        if (!have && lvl1 && __ldg(P.flev + i) == 1) {
-          lev_fwd_row<NS>(A, rr, getr, i, __ldg(P.blev + i), o);
+        if (!have && lvl1 && ldro(P.flev + i) == 1) {
+          lev_fwd_row<NS>(A, rr, getr, i, ldro(P.blev + i), o);
           have = true;
         }
       }
@@ -804,7 +820,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
       };
       if (!precon_tail<NS, NS, T, decltype(rz), CgRows<T>::R>(C, A, (const T *)rn, zw, false, 2, rz)) return false;
     }
-    final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+    final_sum<NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
     unsigned cont = 0;
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
@@ -876,7 +892,7 @@ __device__ __forceinline__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> 
   const KParams &P = *C.P;
   const double BTOL = 1.8189894035458565e-12;   // eps(Float64)^(3/4) = 2^-39
   double red[2 * NS];
-  final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+  final_sum<2 * NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
   const int G1 = w.gmax + 1;
   const int kmax = min(cfg.itmax, w.gmax);
   double *gws = w.gws + (size_t)vbid() * NS * 4 * G1;
@@ -942,7 +958,7 @@ __device__ __forceinline__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> 
         }))
       return false;
     double h[NS];
-    final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, h);
+    final_sum<NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, h);
     if (threadIdx.x == 0)
 #pragma unroll
       for (int d = 0; d < NS; ++d) gws[(size_t)d * 4 * G1 + 3 * G1] = h[d];
@@ -962,7 +978,7 @@ __device__ __forceinline__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> 
         }
       });
       if (!C.sync()) return false;
-      final_sum<NS>(P.part, P.ntiles, C.sm, C.sm_out, h);
+      final_sum<NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, h);
       if (!norm && threadIdx.x == 0)
 #pragma unroll
         for (int d = 0; d < NS; ++d) gws[(size_t)d * 4 * G1 + 3 * G1 + (m - 1)] = h[d];
@@ -1068,14 +1084,14 @@ __device__ __forceinline__ bool krylov(Ctx &C, const MatT<T> &A, const KWorkT<T>
 template <int NS>
 __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax, double (&b)[NS]) {
   const Mat &A = P.AU;
-  const double vol = __ldg(P.vol + i);
+  const double vol = ldro(P.vol + i);
   double acc = 0.0;
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
+    const int f = ldro(P.f_face + e);
     if (f < 0) break;
-    const double ns = (double)__ldg(P.f_sign + e);
-    const int pos = __ldg(P.f_pos + e);
+    const double ns = (double)ldro(P.f_sign + e);
+    const int pos = ldro(P.f_pos + e);
     double t2;
     const double mf = P.mdot[f];
     if (P.div == DIV_UPWIND) {
@@ -1083,21 +1099,21 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
       acc += jmax(ap, 0.0);
       t2 = -jmax(-ap, 0.0);
     } else {
-      const int nb = __ldg(P.f_nbr + e);
-      const double ax = __ldg(P.fcx + f) - __ldg(P.ccx + i), ay = __ldg(P.fcy + f) - __ldg(P.ccy + i),
-                   az = __ldg(P.fcz + f) - __ldg(P.ccz + i);
-      const double bx = __ldg(P.ccx + nb) - __ldg(P.ccx + i), by = __ldg(P.ccy + nb) - __ldg(P.ccy + i),
-                   bz = __ldg(P.ccz + nb) - __ldg(P.ccz + i);
+      const int nb = ldro(P.f_nbr + e);
+      const double ax = ldro(P.fcx + f) - ldro(P.ccx + i), ay = ldro(P.fcy + f) - ldro(P.ccy + i),
+                   az = ldro(P.fcz + f) - ldro(P.ccz + i);
+      const double bx = ldro(P.ccx + nb) - ldro(P.ccx + i), by = ldro(P.ccy + nb) - ldro(P.ccy + i),
+                   bz = ldro(P.ccz + nb) - ldro(P.ccz + i);
       const double weight = sqrt((ax * ax + ay * ay) + az * az) / sqrt((bx * bx + by * by) + bz * bz);
       const double omw = 1.0 - weight;
       const double ap = 1.0 * (mf * ns);
       acc += ap * omw;
       t2 = ap * weight;
     }
-    const double ap3 = -1.0 * ((-P.nueff[f]) * __ldg(P.area + f)) / __ldg(P.delta + f);
+    const double ap3 = -1.0 * ((-P.nueff[f]) * ldro(P.area + f)) / ldro(P.delta + f);
     acc += ap3;
     const double t3 = -ap3;
-    const double base = __ldg(P.f_first + e) ? 0.0 : A.val[pos];
+    const double base = ldro(P.f_first + e) ? 0.0 : A.val[pos];
     A.val[pos] = (base + t2) + t3;
   }
   double prev[NS];
@@ -1112,9 +1128,9 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
 #pragma unroll
   for (int d = 0; d < NS; ++d) b[d] += -1.0 * P.gp[(size_t)i * NS + d] * vol;
   const FieldBC &bc = P.bcU;
-  for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
-    const int f = __ldg(bc.a_face + q);
-    const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+  for (int q = ldro(bc.a_ptr + i); q < ldro(bc.a_ptr + i + 1); ++q) {
+    const int f = ldro(bc.a_face + q);
+    const BcEntry &e = bc.tab[ldro(bc.a_bc + q)];
     const double ap = 1.0 * P.mdot[f];
     if (P.div == DIV_UPWIND) {
       if (e.type == BC_DIRICHLET) {
@@ -1132,7 +1148,7 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
       }
     }
     if (e.type == BC_DIRICHLET) {
-      const double flux = P.nueff[f] * __ldg(P.area + f) / __ldg(P.delta + f);
+      const double flux = P.nueff[f] * ldro(P.area + f) / ldro(P.delta + f);
       const double apl = -1.0 * (-flux);
       acc += apl;
 #pragma unroll
@@ -1144,7 +1160,7 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
 #pragma unroll
     for (int d = 0; d < NS; ++d) b[d] += (1.0 - P.aU) * acc * prev[d];
   }
-  A.val[__ldg(A.dpos + i)] = acc;
+  A.val[ldro(A.dpos + i)] = acc;
   P.rD[i] = vol / acc;
   st<NS>(P.bU, i, b);
 }
@@ -1152,9 +1168,9 @@ __device__ __forceinline__ void momentum_row(const KParams &P, int i, bool relax
 // u . S_f of a face vector field (flux!/div!: psif[fID] . (area*normal))
 template <int NS>
 __device__ __forceinline__ double face_dot_S(const KParams &P, const double *uf, int f) {
-  const double a = __ldg(P.area + f);
-  double s = uf[(size_t)f * NS] * (a * __ldg(P.fnx + f)) + uf[(size_t)f * NS + 1] * (a * __ldg(P.fny + f));
-  if (NS == 3) s = s + uf[(size_t)f * NS + 2] * (a * __ldg(P.fnz + f));
+  const double a = ldro(P.area + f);
+  double s = uf[(size_t)f * NS] * (a * ldro(P.fnx + f)) + uf[(size_t)f * NS + 1] * (a * ldro(P.fny + f));
+  if (NS == 3) s = s + uf[(size_t)f * NS + 2] * (a * ldro(P.fnz + f));
   return s;
 }
 
@@ -1164,36 +1180,36 @@ __device__ __forceinline__ double face_dot_S(const KParams &P, const double *uf,
 template <int NS>
 __device__ __forceinline__ double pressure_row(const KParams &P, int i) {
   const Mat &A = P.AP;
-  const double vol = __ldg(P.vol + i);
+  const double vol = ldro(P.vol + i);
   double dv = 0.0;
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
+    const int f = ldro(P.f_face + e);
     if (f < 0) break;
-    dv += face_dot_S<NS>(P, P.UfH, f) * (double)__ldg(P.f_sign + e) / vol;
+    dv += face_dot_S<NS>(P, P.UfH, f) * (double)ldro(P.f_sign + e) / vol;
   }
-  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q)
-    dv += face_dot_S<NS>(P, P.UfH, __ldg(P.cb_face + q)) / vol;
+  for (int q = ldro(P.cb_ptr + i); q < ldro(P.cb_ptr + i + 1); ++q)
+    dv += face_dot_S<NS>(P, P.UfH, ldro(P.cb_face + q)) / vol;
   P.divH[i] = dv;
   double acc = 0.0;
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
+    const int f = ldro(P.f_face + e);
     if (f < 0) break;
-    const int pos = __ldg(P.f_pos + e);
-    const double ap = 1.0 * ((-P.rDf[f]) * __ldg(P.area + f)) / __ldg(P.delta + f);
+    const int pos = ldro(P.f_pos + e);
+    const double ap = 1.0 * ((-P.rDf[f]) * ldro(P.area + f)) / ldro(P.delta + f);
     acc += ap;
-    const double base = __ldg(P.f_first + e) ? 0.0 : A.val[pos];
+    const double base = ldro(P.f_first + e) ? 0.0 : A.val[pos];
     A.val[pos] = base + (-ap);
   }
   double b = 0.0;
   b += 1.0 * dv * vol;
   const FieldBC &bc = P.bcP;
-  for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
-    const int f = __ldg(bc.a_face + q);
-    const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+  for (int q = ldro(bc.a_ptr + i); q < ldro(bc.a_ptr + i + 1); ++q) {
+    const int f = ldro(bc.a_face + q);
+    const BcEntry &e = bc.tab[ldro(bc.a_bc + q)];
     if (e.type == BC_DIRICHLET) {
-      const double flux = P.rDf[f] * __ldg(P.area + f) / __ldg(P.delta + f);
+      const double flux = P.rDf[f] * ldro(P.area + f) / ldro(P.delta + f);
       const double ap = 1.0 * (-flux);
       acc += ap;
       b += ap * e.v[0];
@@ -1203,7 +1219,7 @@ __device__ __forceinline__ double pressure_row(const KParams &P, int i) {
     b += acc * P.pref;
     acc += acc;
   }
-  A.val[__ldg(A.dpos + i)] = acc;
+  A.val[ldro(A.dpos + i)] = acc;
   P.bP[i] = b;
   return b;
 }
@@ -1218,14 +1234,14 @@ __device__ __forceinline__ void H_row(const KParams &P, int i, const double (&bb
   for (int d = 0; d < NS; ++d) sum[d] = 0.0;
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
+    const int f = ldro(P.f_face + e);
     if (f < 0) break;
-    const int nb = __ldg(P.f_nbr + e);
-    const double a = A.val[__ldg(P.f_pos + e)];
+    const int nb = ldro(P.f_nbr + e);
+    const double a = A.val[ldro(P.f_pos + e)];
 #pragma unroll
     for (int d = 0; d < NS; ++d) sum[d] += a * P.U[(size_t)nb * NS + d];
   }
-  const double rDc = 1 / A.val[__ldg(A.dpos + i)];
+  const double rDc = 1 / A.val[ldro(A.dpos + i)];
 #pragma unroll
   for (int d = 0; d < NS; ++d) P.H[(size_t)i * NS + d] = (bb[d] - sum[d]) * rDc;
 }
@@ -1235,13 +1251,13 @@ __device__ __forceinline__ void H_row(const KParams &P, int i, const double (&bb
 // (:135-237) for a vector cell field.
 template <int NS>
 __device__ __forceinline__ void face_vector(const KParams &P, const double *cellv, int f, double (&u)[NS]) {
-  const double w = __ldg(P.wgt + f);
+  const double w = ldro(P.wgt + f);
   const double omw = 1.0 - w;
-  const int a = __ldg(P.o1 + f), b = __ldg(P.o2 + f);
+  const int a = ldro(P.o1 + f), b = ldro(P.o2 + f);
 #pragma unroll
   for (int d = 0; d < NS; ++d) u[d] = w * cellv[(size_t)a * NS + d] + omw * cellv[(size_t)b * NS + d];
   if (f < P.nbf) {
-    const int bi = __ldg(P.bcU.fbc + f);
+    const int bi = ldro(P.bcU.fbc + f);
     if (bi >= 0) {
       const BcEntry &e = P.bcU.tab[bi];
 #pragma unroll
@@ -1258,9 +1274,9 @@ __device__ __forceinline__ void face_mdot(const KParams &P, int f) {
   if (P.model == 1)
 #pragma unroll
     for (int d = 0; d < NS; ++d) P.UfH[(size_t)f * NS + d] = u[d];
-  const double a = __ldg(P.area + f);
-  double m = u[0] * (a * __ldg(P.fnx + f)) + u[1] * (a * __ldg(P.fny + f));
-  if (NS == 3) m = m + u[2] * (a * __ldg(P.fnz + f));
+  const double a = ldro(P.area + f);
+  double m = u[0] * (a * ldro(P.fnx + f)) + u[1] * (a * ldro(P.fny + f));
+  if (NS == 3) m = m + u[2] * (a * ldro(P.fnz + f));
   P.mdot[f] = m;
 }
 
@@ -1268,16 +1284,16 @@ __device__ __forceinline__ void face_mdot(const KParams &P, int f) {
 template <int NS>
 __device__ __forceinline__ double midpoint_corrected(const KParams &P, int f) {
   const double w = 0.5;
-  const int a = __ldg(P.o1 + f), b = __ldg(P.o2 + f);
+  const int a = ldro(P.o1 + f), b = ldro(P.o2 + f);
   const double phifp = w * (P.p[a] + P.p[b]);
   const double g0 = w * (P.gp[(size_t)a * NS] + P.gp[(size_t)b * NS]);
   const double g1 = w * (P.gp[(size_t)a * NS + 1] + P.gp[(size_t)b * NS + 1]);
-  const double r0 = __ldg(P.fcx + f) - w * (__ldg(P.ccx + a) + __ldg(P.ccx + b));
-  const double r1 = __ldg(P.fcy + f) - w * (__ldg(P.ccy + a) + __ldg(P.ccy + b));
+  const double r0 = ldro(P.fcx + f) - w * (ldro(P.ccx + a) + ldro(P.ccx + b));
+  const double r1 = ldro(P.fcy + f) - w * (ldro(P.ccy + a) + ldro(P.ccy + b));
   double dt = g0 * r0 + g1 * r1;
   if (NS == 3) {
     const double g2 = w * (P.gp[(size_t)a * NS + 2] + P.gp[(size_t)b * NS + 2]);
-    const double r2 = __ldg(P.fcz + f) - w * (__ldg(P.ccz + a) + __ldg(P.ccz + b));
+    const double r2 = ldro(P.fcz + f) - w * (ldro(P.ccz + a) + ldro(P.ccz + b));
     dt = dt + g2 * r2;
   }
   return phifp + dt;
@@ -1338,14 +1354,14 @@ __device__ __forceinline__ double omega_wall(const KParams &P, const BcEntry &e,
 __device__ __forceinline__ double scalar_row(const KParams &P, const Mat &A, int i, const double *phi,
                                              const double *gam, const double *Si, const double *src,
                                              const FieldBC &bc, double alpha, int div, int time, bool omega) {
-  const double vol = __ldg(P.vol + i);
+  const double vol = ldro(P.vol + i);
   double acc = 0.0;
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
+    const int f = ldro(P.f_face + e);
     if (f < 0) break;
-    const double ns = (double)__ldg(P.f_sign + e);
-    const int pos = __ldg(P.f_pos + e);
+    const double ns = (double)ldro(P.f_sign + e);
+    const int pos = ldro(P.f_pos + e);
     double t2;
     const double mf = P.mdot[f];
     if (div == DIV_UPWIND) {
@@ -1353,21 +1369,21 @@ __device__ __forceinline__ double scalar_row(const KParams &P, const Mat &A, int
       acc += jmax(ap, 0.0);
       t2 = -jmax(-ap, 0.0);
     } else {
-      const int nb = __ldg(P.f_nbr + e);
-      const double ax = __ldg(P.fcx + f) - __ldg(P.ccx + i), ay = __ldg(P.fcy + f) - __ldg(P.ccy + i),
-                   az = __ldg(P.fcz + f) - __ldg(P.ccz + i);
-      const double bx = __ldg(P.ccx + nb) - __ldg(P.ccx + i), by = __ldg(P.ccy + nb) - __ldg(P.ccy + i),
-                   bz = __ldg(P.ccz + nb) - __ldg(P.ccz + i);
+      const int nb = ldro(P.f_nbr + e);
+      const double ax = ldro(P.fcx + f) - ldro(P.ccx + i), ay = ldro(P.fcy + f) - ldro(P.ccy + i),
+                   az = ldro(P.fcz + f) - ldro(P.ccz + i);
+      const double bx = ldro(P.ccx + nb) - ldro(P.ccx + i), by = ldro(P.ccy + nb) - ldro(P.ccy + i),
+                   bz = ldro(P.ccz + nb) - ldro(P.ccz + i);
       const double weight = sqrt((ax * ax + ay * ay) + az * az) / sqrt((bx * bx + by * by) + bz * bz);
       const double omw = 1.0 - weight;
       const double ap = 1.0 * (mf * ns);
       acc += ap * omw;
       t2 = ap * weight;
     }
-    const double ap3 = -1.0 * ((-gam[f]) * __ldg(P.area + f)) / __ldg(P.delta + f);
+    const double ap3 = -1.0 * ((-gam[f]) * ldro(P.area + f)) / ldro(P.delta + f);
     acc += ap3;
     const double t3 = -ap3;
-    const double base = __ldg(P.f_first + e) ? 0.0 : A.val[pos];
+    const double base = ldro(P.f_first + e) ? 0.0 : A.val[pos];
     A.val[pos] = (base + t2) + t3;
   }
   const double prev = phi[i];
@@ -1379,9 +1395,9 @@ __device__ __forceinline__ double scalar_row(const KParams &P, const Mat &A, int
   }
   acc += 1.0 * Si[i] * vol;
   b += 1.0 * src[i] * vol;
-  for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
-    const int f = __ldg(bc.a_face + q);
-    const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+  for (int q = ldro(bc.a_ptr + i); q < ldro(bc.a_ptr + i + 1); ++q) {
+    const int f = ldro(bc.a_face + q);
+    const BcEntry &e = bc.tab[ldro(bc.a_bc + q)];
     const double ap = 1.0 * P.mdot[f];
     const bool neu = (e.type == BC_NEUMANN || e.type == BC_KWALL || e.type == BC_OMEGAWALL);
     if (div == DIV_UPWIND) {
@@ -1392,7 +1408,7 @@ __device__ __forceinline__ double scalar_row(const KParams &P, const Mat &A, int
       else if (neu) acc += ap;
     }
     if (e.type == BC_DIRICHLET) {
-      const double flux = gam[f] * __ldg(P.area + f) / __ldg(P.delta + f);
+      const double flux = gam[f] * ldro(P.area + f) / ldro(P.delta + f);
       const double apl = -1.0 * (-flux);
       acc += apl;
       b += apl * e.v[0];
@@ -1405,14 +1421,14 @@ __device__ __forceinline__ double scalar_row(const KParams &P, const Mat &A, int
   acc /= alpha;
   b += (1.0 - alpha) * acc * prev;
   if (omega)
-    for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
-      const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+    for (int q = ldro(bc.a_ptr + i); q < ldro(bc.a_ptr + i + 1); ++q) {
+      const BcEntry &e = bc.tab[ldro(bc.a_bc + q)];
       if (e.type != BC_OMEGAWALL) continue;
-      const double wc = omega_wall(P, e, P.k[i], __ldg(P.delta + __ldg(bc.a_face + q)));
+      const double wc = omega_wall(P, e, P.k[i], ldro(P.delta + ldro(bc.a_face + q)));
       b += acc * wc;
       acc += acc;
     }
-  A.val[__ldg(A.dpos + i)] = acc;
+  A.val[ldro(A.dpos + i)] = acc;
   return b;
 }
 
@@ -1426,11 +1442,11 @@ __device__ __forceinline__ void grad_u_row(const KParams &P, int i, double (&g)[
     for (int j = 0; j < 3; ++j) g[d][j] = 0.0;
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    const int f = __ldg(P.f_face + e);
+    const int f = ldro(P.f_face + e);
     if (f < 0) break;
-    const double ns = (double)__ldg(P.f_sign + e);
-    const double a = __ldg(P.area + f);
-    const double sx = (a * __ldg(P.fnx + f)) * ns, sy = (a * __ldg(P.fny + f)) * ns, sz = (a * __ldg(P.fnz + f)) * ns;
+    const double ns = (double)ldro(P.f_sign + e);
+    const double a = ldro(P.area + f);
+    const double sx = (a * ldro(P.fnx + f)) * ns, sy = (a * ldro(P.fny + f)) * ns, sz = (a * ldro(P.fnz + f)) * ns;
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
       const double v = P.UfH[(size_t)f * NS + d];
@@ -1439,15 +1455,15 @@ __device__ __forceinline__ void grad_u_row(const KParams &P, int i, double (&g)[
       if (NS == 3) g[d][2] += v * sz;
     }
   }
-  const double vol = __ldg(P.vol + i);
+  const double vol = ldro(P.vol + i);
 #pragma unroll
   for (int d = 0; d < NS; ++d)
 #pragma unroll
     for (int j = 0; j < NS; ++j) g[d][j] /= vol;
-  for (int q = __ldg(P.cb_ptr + i); q < __ldg(P.cb_ptr + i + 1); ++q) {
-    const int f = __ldg(P.cb_face + q);
-    const double a = __ldg(P.area + f);
-    const double sx = a * __ldg(P.fnx + f), sy = a * __ldg(P.fny + f), sz = a * __ldg(P.fnz + f);
+  for (int q = ldro(P.cb_ptr + i); q < ldro(P.cb_ptr + i + 1); ++q) {
+    const int f = ldro(P.cb_face + q);
+    const double a = ldro(P.area + f);
+    const double sx = a * ldro(P.fnx + f), sy = a * ldro(P.fny + f), sz = a * ldro(P.fnz + f);
 #pragma unroll
     for (int d = 0; d < NS; ++d) {
       const double v = P.UfH[(size_t)f * NS + d];
@@ -1473,8 +1489,8 @@ __device__ __forceinline__ void bound_row(const KParams &P, double *fld, int i) 
   int cnt = 0;
   for (int k = 0; k < P.Wf; ++k) {
     const size_t e = (size_t)k * P.np + i;
-    if (__ldg(P.f_face + e) < 0) break;
-    sum_flux += jmax(fld[__ldg(P.f_nbr + e)], EPS);
+    if (ldro(P.f_face + e) < 0) break;
+    sum_flux += jmax(fld[ldro(P.f_nbr + e)], EPS);
     cnt += 1;
   }
   const double average = sum_flux / (double)cnt;
@@ -1510,12 +1526,12 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
     P.Dk[i] = KW_BPLUS * wi;
     double pki = P.nut[i] * pk;
     const FieldBC &bc = P.bcK;
-    for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {   // correct_production!
-      const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+    for (int q = ldro(bc.a_ptr + i); q < ldro(bc.a_ptr + i + 1); ++q) {   // correct_production!
+      const BcEntry &e = bc.tab[ldro(bc.a_bc + q)];
       if (e.type != BC_KWALL) continue;
-      const int f = __ldg(bc.a_face + q);
-      const double delta = __ldg(P.delta + f);
-      const double nx = __ldg(P.fnx + f), ny = __ldg(P.fny + f), nz = __ldg(P.fnz + f);
+      const int f = ldro(bc.a_face + q);
+      const double delta = ldro(P.delta + f);
+      const double nx = ldro(P.fnx + f), ny = ldro(P.fny + f), nz = ldro(P.fnz + f);
       const double kc = P.k[i];
       const double uStar = e.c25 * sqrt(kc);
       const double dUdy = uStar / (e.kappa * delta);
@@ -1561,10 +1577,10 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
       double v = (double)wk.x[i] + phi[i];
       if (om) {
         const FieldBC &bc = P.bcW;
-        for (int q = __ldg(bc.a_ptr + i); q < __ldg(bc.a_ptr + i + 1); ++q) {
-          const BcEntry &e = bc.tab[__ldg(bc.a_bc + q)];
+        for (int q = ldro(bc.a_ptr + i); q < ldro(bc.a_ptr + i + 1); ++q) {
+          const BcEntry &e = bc.tab[ldro(bc.a_bc + q)];
           if (e.type != BC_OMEGAWALL) continue;
-          v = omega_wall(P, e, P.k[i], __ldg(P.delta + __ldg(bc.a_face + q)));
+          v = omega_wall(P, e, P.k[i], ldro(P.delta + ldro(bc.a_face + q)));
         }
       }
       phi[i] = v;
@@ -1572,7 +1588,7 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
     if (!C.sync()) return false;
     for (int l = 0; l < P.nfl; ++l) {   // bound!(phi, eps()); after k also nut = k/omega
       tile_each(P, [&](int i) {
-        if (__ldg(P.flev + i) != l) return;
+        if (ldro(P.flev + i) != l) return;
         bound_row(P, phi, i);
         if (!om) P.nut[i] = P.k[i] / P.w[i];
       });
@@ -1585,11 +1601,11 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
   grid_each(P.nf, [&](int f) {
     double v = face_scalar(P, P.nut, f, P.bcN, false);
     if (f < P.nbf) {
-      const int bi = __ldg(P.bcN.fbc + f);
+      const int bi = ldro(P.bcN.fbc + f);
       if (bi >= 0 && P.bcN.tab[bi].type == BC_NUTWALL) {
         const BcEntry &e = P.bcN.tab[bi];
-        const int c = __ldg(P.o1 + f);
-        const double yplus = e.c25 * __ldg(P.delta + f) * sqrt(P.k[c]) / nu;
+        const int c = ldro(P.o1 + f);
+        const double yplus = e.c25 * ldro(P.delta + f) * sqrt(P.k[c]) / nu;
         const double nutw = nut_wall_fn(nu, yplus, e.kappa, e.E);
         if (yplus > e.ylam) v = nutw;
       }
@@ -1653,7 +1669,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
     tile_phase<2 * NS>(C, true, [&](int i, double (&v)[2 * NS]) {
       double y[NS], bb[NS];
       spmv_row<NS>(P.AU, i, [&](int j, int d) { return P.U[(size_t)j * NS + d]; }, y);
-      const double vol = __ldg(P.vol + i);
+      const double vol = ldro(P.vol + i);
       ld<NS>(P.bU, i, bb);
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
@@ -1668,7 +1684,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
     if (!C.sync()) return;
     {
       double red[2 * NS];
-      final_sum<2 * NS>(P.part, P.ntiles, C.sm, C.sm_out, red);
+      final_sum<2 * NS>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
 #pragma unroll
       for (int d = 0; d < NS; ++d) Rit[d] = sqrt(red[2 * d] / (double)P.n) / sqrt(red[2 * d + 1]);
       if (vbid() == 0 && threadIdx.x == 0) {
@@ -1693,9 +1709,9 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
       // interpolate!(rDf, rD); interpolate!(Uf, Hv) + correct_boundaries!
       C.phase(PH_FACE);
       grid_each(P.nf, [&](int f) {
-        const double w = __ldg(P.wgt + f);
+        const double w = ldro(P.wgt + f);
         const double omw = 1.0 - w;
-        P.rDf[f] = w * P.rD[__ldg(P.o1 + f)] + omw * P.rD[__ldg(P.o2 + f)];
+        P.rDf[f] = w * P.rD[ldro(P.o1 + f)] + omw * P.rD[ldro(P.o2 + f)];
         double u[NS];
         face_vector<NS>(P, P.H, f, u);
 #pragma unroll
@@ -1739,7 +1755,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
       if (!C.sync()) return;
       {
         double red[2];
-        final_sum<2>(P.part, P.ntiles, C.sm, C.sm_out, red);
+        final_sum<2>(C.part_r(), P.ntiles, C.sm, C.sm_out, red);
         Rit[3] = sqrt(red[0] / (double)P.n) / sqrt(red[1]);
         if (vbid() == 0 && threadIdx.x == 0) {
           P.R[(size_t)it * 4 + 3] = Rit[3];
@@ -1832,6 +1848,8 @@ __global__ void __launch_bounds__(TPB, MB) xcal_program_kernel(const __grid_cons
   C.S.timeout_ns = prm.bar_timeout_ns ? prm.bar_timeout_ns : BARRIER_TIMEOUT_NS;
   C.S.epoch = 0;
   C.S.ok = &sm_ok;
+  C.part = prm.part;
+  C.pw = 0;
   C.sm = sm;
   C.sm_out = sm_out;
   C.ws = ws;
@@ -1882,9 +1900,10 @@ __global__ void __launch_bounds__(TPB, MB) xcal_serve_kernel(ServeMail *mail, co
   __shared__ double ws[MAXTL * MAXK * 8];
   __shared__ int sm_ok;
   __shared__ unsigned long long pacc[2 * NPH];
-  __shared__ KParams sP;
-  __shared__ ServeJob *s_job;
+  __shared__ ServeJob sJ;   // the job record, read once per job
+  __shared__ const ServeJob *s_job;
   __shared__ int s_cmd;
+  static_assert(sizeof(ServeJob) % 8 == 0, "job record copied in 8-byte words");
   ServeMail *m = mail + blockIdx.x;
   unsigned long long seen = 0;
   if (threadIdx.x == 0) seen = *(volatile unsigned long long *)&m->ack;
@@ -1916,31 +1935,36 @@ __global__ void __launch_bounds__(TPB, MB) xcal_serve_kernel(ServeMail *mail, co
         if (nap < 32768u) nap <<= 1;
       }
       if (cmd) {
-        s_job = m->job;
-        s_vbid = m->vbid;
-        s_vnb = m->nblk;
+        // mail fields through volatile loads: the same words held earlier
+        // jobs' values, which this SM may still have cached
+        s_job = *(ServeJob *const volatile *)&m->job;
+        s_vbid = *(volatile const int *)&m->vbid;
+        s_vnb = *(volatile const int *)&m->nblk;
         *(volatile unsigned long long *)&m->ack = seen;
       }
       s_cmd = cmd;
     }
     __syncthreads();
     if (!s_cmd) return;
-    ServeJob *J = s_job;
-    // the case's parameters into shared memory (read once over the bus)
+    // The job record and the case image live in pinned host memory whose
+    // regions are reused by later jobs: read them with ld.global.cv (fetch
+    // again, never from a cached line).
     {
-      const unsigned long long *src = (const unsigned long long *)&J->prm;
-      unsigned long long *dst = (unsigned long long *)&sP;
-      for (int k = threadIdx.x; k < (int)(sizeof(KParams) / 8); k += TPB) dst[k] = src[k];
+      const unsigned long long *src = (const unsigned long long *)s_job;
+      unsigned long long *dst = (unsigned long long *)&sJ;
+      for (int k = threadIdx.x; k < (int)(sizeof(ServeJob) / 8); k += TPB) dst[k] = __ldcv(src + k);
     }
     __syncthreads();
+    const ServeJob &J = sJ;
+    const KParams &sP = sJ.prm;
     const int B = vbid(), G = vnb();
     // this CTA's share of the region: image copy, then zero part
     {
-      const uint4 *src = J->src;
-      uint4 *dst = J->dst;
-      const unsigned long long c16 = J->copy16, z16 = J->zero16;
+      const uint4 *src = J.src;
+      uint4 *dst = J.dst;
+      const unsigned long long c16 = J.copy16, z16 = J.zero16;
       for (unsigned long long q = (unsigned long long)B * TPB + threadIdx.x; q < c16; q += (unsigned long long)G * TPB)
-        dst[q] = src[q];
+        dst[q] = __ldcv(src + q);
       const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
       for (unsigned long long q = (unsigned long long)B * TPB + threadIdx.x; q < z16; q += (unsigned long long)G * TPB)
         dst[c16 + q] = zero;
@@ -1954,6 +1978,8 @@ __global__ void __launch_bounds__(TPB, MB) xcal_serve_kernel(ServeMail *mail, co
     C.S.timeout_ns = BARRIER_TIMEOUT_NS;
     C.S.epoch = 0;
     C.S.ok = &sm_ok;
+    C.part = sP.part;
+    C.pw = 0;
     C.sm = sm;
     C.sm_out = sm_out;
     C.ws = ws;
@@ -1961,34 +1987,34 @@ __global__ void __launch_bounds__(TPB, MB) xcal_serve_kernel(ServeMail *mail, co
     C.tag = PH_SETUP;
     C.pacc = pacc;
     C.t_last = 0;
-    if (C.sync()) simple_program<NS, T>(C, J->iters, J->prog == PROG_PISO);
+    if (C.sync()) simple_program<NS, T>(C, J.iters, J.prog == PROG_PISO);
     C.sync();   // the run's results (fields, histories, done) complete
     // results to pinned host memory, this CTA's share
     {
       const int n = sP.n;
       const int dn = *(volatile const int *)sP.done;
-      for (int q = B * TPB + threadIdx.x; q < n * NS; q += G * TPB) J->out_U[q] = sP.U[q];
-      for (int q = B * TPB + threadIdx.x; q < n; q += G * TPB) J->out_p[q] = sP.p[q];
-      for (int q = B * TPB + threadIdx.x; q < dn * 4; q += G * TPB) J->out_R[q] = sP.R[q];
-      for (int q = B * TPB + threadIdx.x; q < dn * 5; q += G * TPB) J->out_kry[q] = sP.kry[q];
+      for (int q = B * TPB + threadIdx.x; q < n * NS; q += G * TPB) J.out_U[q] = sP.U[q];
+      for (int q = B * TPB + threadIdx.x; q < n; q += G * TPB) J.out_p[q] = sP.p[q];
+      for (int q = B * TPB + threadIdx.x; q < dn * 4; q += G * TPB) J.out_R[q] = sP.R[q];
+      for (int q = B * TPB + threadIdx.x; q < dn * 5; q += G * TPB) J.out_kry[q] = sP.kry[q];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence_system();
-      const unsigned prev = atom_add_acqrel_u32(J->exits, 1u);
+      const unsigned prev = atom_add_acqrel_u32(J.exits, 1u);
       if (prev + 1u == (unsigned)G) {
         // last CTA of the group out: state for the host, then the group's
         // barrier word and exit count reset for the next case that uses them
         volatile Bar *b = sP.bar;
-        J->out_state[0] = *(volatile const int *)sP.done;
-        J->out_state[1] = b->err;
-        J->out_state[2] = b->nonfinite;
+        J.out_state[0] = *(volatile const int *)sP.done;
+        J.out_state[1] = b->err;
+        J.out_state[2] = b->nonfinite;
         b->count = 0ull;
         b->err = 0;
         b->nonfinite = 0;
-        *(volatile unsigned *)J->exits = 0u;
+        *(volatile unsigned *)J.exits = 0u;
         __threadfence_system();
-        st_release_sys_i32(J->out_state + 3, 1);
+        st_release_sys_i32(J.out_state + 3, 1);
       }
     }
     __syncthreads();

@@ -96,6 +96,7 @@ struct RangeAlloc {
 };
 
 size_t up256(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t SLOT_BYTES = 128;
 
 struct Job {
   int64_t ticket = 0;
@@ -133,8 +134,8 @@ struct xcal_server_s {
   char *dev_arena = nullptr;
   char *host_arena = nullptr, *host_arena_dev = nullptr;
   RangeAlloc dalloc, halloc;
-  xcal::Bar *bars = nullptr;
-  unsigned *exits = nullptr;
+  // per slot, one 128-byte line: the group's barrier word, then its exit count
+  char *slotmem = nullptr;
   std::vector<int> free_slots;
   // control records in pinned host memory
   ServeMail *mail = nullptr, *mail_dev = nullptr;
@@ -355,8 +356,8 @@ void post(xcal_server s, Job &j) {
   const int slot = s->free_slots.back();
   s->free_slots.pop_back();
   j.slot = slot;
-  j.sj->prm.bar = s->bars + slot;
-  j.sj->exits = s->exits + slot;
+  j.sj->prm.bar = (xcal::Bar *)(s->slotmem + SLOT_BYTES * slot);
+  j.sj->exits = (unsigned *)(s->slotmem + SLOT_BYTES * slot + 64);
   j.ctas.clear();
   for (int c = 0; c < s->grid && (int)j.ctas.size() < j.k; ++c)
     if (!s->cta_busy[c]) {
@@ -450,8 +451,7 @@ int launch_server_kernel(xcal_server s) {
 void release_resources(xcal_server s) {
   if (s->kstream) cudaStreamSynchronize(s->kstream);
   if (s->dev_arena) cudaFree(s->dev_arena);
-  if (s->bars) cudaFree(s->bars);
-  if (s->exits) cudaFree(s->exits);
+  if (s->slotmem) cudaFree(s->slotmem);
   if (s->host_arena) cudaFreeHost(s->host_arena);
   if (s->mail) cudaFreeHost(s->mail);
   if (s->ctl) cudaFreeHost(s->ctl);
@@ -494,12 +494,11 @@ int xcal_serve_create(int device, const xcal_serve_cfg *cfg, xcal_server *out) {
     return XCAL_ERR_CUDA;
   }
   size_t dbytes = cfg->device_bytes > 0.0 ? (size_t)cfg->device_bytes : (size_t)(0.5 * (double)freeb);
-  dbytes = std::min(up256(dbytes), (size_t)(0.9 * (double)freeb)) / 256 * 256;
+  dbytes = std::min(dbytes, (size_t)(0.9 * (double)freeb)) / 256 * 256;   // never more than asked for
   const size_t hbytes = up256(cfg->host_bytes > 0.0 ? (size_t)cfg->host_bytes : ((size_t)4 << 30));
   const int nslots = std::min(cfg->slots, s->grid);
   bool ok = cudaMalloc(&s->dev_arena, dbytes) == cudaSuccess &&
-            cudaMalloc(&s->bars, sizeof(xcal::Bar) * nslots) == cudaSuccess &&
-            cudaMalloc(&s->exits, sizeof(unsigned) * nslots) == cudaSuccess &&
+            cudaMalloc(&s->slotmem, SLOT_BYTES * nslots) == cudaSuccess &&
             cudaHostAlloc(&s->host_arena, hbytes, cudaHostAllocMapped | cudaHostAllocPortable) == cudaSuccess &&
             cudaHostAlloc(&s->mail, sizeof(ServeMail) * s->grid, cudaHostAllocMapped | cudaHostAllocPortable) ==
                 cudaSuccess &&
@@ -516,8 +515,7 @@ int xcal_serve_create(int device, const xcal_serve_cfg *cfg, xcal_server *out) {
     s->ctl_dev = (ServeCtl *)p;
   }
   if (ok) {
-    ok = cudaMemsetAsync(s->bars, 0, sizeof(xcal::Bar) * nslots, s->kstream) == cudaSuccess &&
-         cudaMemsetAsync(s->exits, 0, sizeof(unsigned) * nslots, s->kstream) == cudaSuccess &&
+    ok = cudaMemsetAsync(s->slotmem, 0, SLOT_BYTES * nslots, s->kstream) == cudaSuccess &&
          cudaStreamSynchronize(s->kstream) == cudaSuccess;
   }
   if (!ok) {
