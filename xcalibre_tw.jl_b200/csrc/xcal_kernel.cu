@@ -299,26 +299,36 @@ __device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *i
   C.phase(setup ? PH_PREC_SETUP : PH_KRY_PREC);
   if constexpr (R > 1) {
     if (!setup && A.precon == PRECON_DILU && nph > 0) {
-      // the DILU levels R rows at a time; rows outside the level compute
-      // with what they read and store nothing
+      // the DILU levels R rows at a time; in a warp holding a row of the
+      // level, rows outside it compute with what they read and store
+      // nothing; a warp without one skips the rows (with a level-ordered
+      // numbering whole tiles lie outside each level)
       int ph = 0;
       for (int l = first_lvl; l < P.nfl; ++l) {
         const bool last = (++ph == nph);
         tile_phase_rows<K, R>(C, last, [&](const int (&ii)[R], const bool (&ok)[R], double (&v)[R][K]) {
-          T iv[R][NS], o[R][NS];
-          int bl[R];
+          bool at[R], any = false;
 #pragma unroll
           for (int r = 0; r < R; ++r) {
-            bl[r] = ldro(P.blev + ii[r]);
-#pragma unroll
-            for (int d = 0; d < NS; ++d) iv[r][d] = in[(size_t)ii[r] * NS + d];
+            at[r] = ok[r] && ldro(P.flev + ii[r]) == l;
+            any = any || at[r];
           }
-          dilu_fwd_rows<R, NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, ii, bl, o);
+          if (__any_sync(0xffffffffu, any)) {
+            T iv[R][NS], o[R][NS];
+            int bl[R];
 #pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (ok[r] && ldro(P.flev + ii[r]) == l)
+            for (int r = 0; r < R; ++r) {
+              bl[r] = ldro(P.blev + ii[r]);
 #pragma unroll
-              for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
+              for (int d = 0; d < NS; ++d) iv[r][d] = in[(size_t)ii[r] * NS + d];
+            }
+            dilu_fwd_rows<R, NS>(A, iv, [&](int j, int d) { return out[(size_t)j * NS + d]; }, ii, bl, o);
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              if (at[r])
+#pragma unroll
+                for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
+          }
           if (last)
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -329,13 +339,21 @@ __device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *i
       for (int l = 1; l < P.nbl; ++l) {
         const bool last = (++ph == nph);
         tile_phase_rows<K, R>(C, last, [&](const int (&ii)[R], const bool (&ok)[R], double (&v)[R][K]) {
-          T o[R][NS];
-          dilu_bwd_rows<R, NS>(A, out, ii, o);
+          bool at[R], any = false;
 #pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (ok[r] && ldro(P.blev + ii[r]) == l)
+          for (int r = 0; r < R; ++r) {
+            at[r] = ok[r] && ldro(P.blev + ii[r]) == l;
+            any = any || at[r];
+          }
+          if (__any_sync(0xffffffffu, any)) {
+            T o[R][NS];
+            dilu_bwd_rows<R, NS>(A, out, ii, o);
 #pragma unroll
-              for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
+            for (int r = 0; r < R; ++r)
+              if (at[r])
+#pragma unroll
+                for (int d = 0; d < NS; ++d) out[(size_t)ii[r] * NS + d] = o[r][d];
+          }
           if (last)
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -753,7 +771,26 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
               }
             }
           }
-          dilu_fwd_rows<R, NS>(A, rr, getr, ii, bl, o);
+          // only level-1 rows have lower neighbours to sum over; a warp
+          // without one takes the row-local step (level 0: o = r, scaled by
+          // the pivot's inverse when the row has no upper neighbours)
+          bool any = false;
+#pragma unroll
+          for (int r = 0; r < R; ++r) any = any || (ok[r] && lvl1 && fl[r] == 1);
+          if (__any_sync(0xffffffffu, any)) {
+            dilu_fwd_rows<R, NS>(A, rr, getr, ii, bl, o);
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+#pragma unroll
+              for (int d = 0; d < NS; ++d) o[r][d] = rr[r][d];
+              if (bl[r] == 0) {
+                const T di = A.Dinv[ii[r]];
+#pragma unroll
+                for (int d = 0; d < NS; ++d) o[r][d] = o[r][d] * di;
+              }
+            }
+          }
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             if (!ok[r]) continue;
