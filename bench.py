@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip xcal_autotune (the launch form of the library's heuristic is timed)")
     return ap.parse_args()
 
 
@@ -631,6 +633,9 @@ def main():
         s = X.Solver(mesh, device=local if world > 1 else 0, renumber=renum, flags=_abi.FLAG_PHASE_TIMERS)
         s.setup(case)
         reset(s)
+        # the library's autotuner picks the launch form (untimed set-up; every
+        # form computes the same values)
+        tune = None if a.no_tune else s.autotune(3)
         for _ in range(max(a.warmup, 0)):
             s.run(1, want_krylov=False)
         reset(s)
@@ -643,7 +648,7 @@ def main():
         total_ms = max_over_ranks(float(ms.sum()), dist, dev)
         sk = 4 if prec == _abi.PREC_MIXED else 8
         table, total_bytes = phase_table(mesh, ns, sk, ms, kry, ph, peak)
-        runs[name] = dict(ms=ms, kry=kry, total_ms=total_ms, fields=fields, phases=table,
+        runs[name] = dict(ms=ms, kry=kry, total_ms=total_ms, fields=fields, phases=table, tune=tune,
                           bytes_per_step=total_bytes / a.steps,
                           value=job_throughput(world, N * a.steps, total_ms / 1000.0))
         if solver_keep is None:
@@ -709,6 +714,7 @@ def main():
                      "peak_kind": peak_kind, "traffic": load_traffic(f"{a.config}_{N}_{main_name}_simple"),
                      "kernel": "xcal_program_kernel (persistent SIMPLE iteration)"},
         "phases": {k: v["phases"] for k, v in runs.items()},
+        "autotune": {k: v["tune"] for k, v in runs.items()},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps, "precision": main_name},

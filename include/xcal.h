@@ -391,7 +391,7 @@ typedef struct {
   int32_t precision;        /* XCAL_PREC_* of every case */
   double tolerance;         /* stop when all residuals <= tolerance */
   int32_t dim;              /* mesh dimension of every case: 2 or 3 */
-  int32_t tiles_per_cta;    /* CTA group sizing (0: 2) */
+  int32_t tiles_per_cta;    /* CTA group sizing (0: 4) */
   int32_t max_ctas;         /* largest CTA group of one case (0: 64) */
   int32_t setup_threads;    /* host threads laying cases out (0: half the cores, 2..8) */
   double device_bytes;      /* device arena, the admission budget (0: half the free memory) */

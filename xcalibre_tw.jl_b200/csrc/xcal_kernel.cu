@@ -71,8 +71,14 @@ struct Ctx {
   int tag;
   long long t_last;
   unsigned long long *pacc;   // shared [2*NPH]: cycles, counts
+  // Traversal direction of the tile loops, reversed at every barrier: a phase
+  // then starts on the tiles the previous phase touched last, whose data are
+  // the most likely still in L2 when the working set is larger than L2.  Every
+  // row's values are independent of the order, so results are unchanged.
+  int rev;
   __device__ __forceinline__ void phase(int t) { tag = t; }
   __device__ __forceinline__ bool sync() {
+    rev ^= 1;
     const bool ok = S.sync();
     if (timers) {
       const long long t = clock64();
@@ -102,10 +108,22 @@ __device__ __forceinline__ const KWorkT<T> &workP(const KParams &P) {
 }
 
 // ---------------------------------------------------------------- phases
+// The CTA's tiles are vbid(), vbid() + vnb(), ...: own_tiles of them, the
+// m-th in the phase's traversal direction being own_tile(m).
+__device__ __forceinline__ int own_tiles(int nt) {
+  const int B = vbid(), G = vnb();
+  return B < nt ? (nt - 1 - B) / G + 1 : 0;
+}
+__device__ __forceinline__ int own_tile(int m, int cnt, int rev) {
+  return vbid() + vnb() * (rev ? cnt - 1 - m : m);
+}
+
 template <class F>
-__device__ __forceinline__ void tile_each(const KParams &P, F f) {
-  for (int t = vbid(); t < P.ntiles; t += vnb()) {
-    const int i = t * TILE + threadIdx.x;
+__device__ __forceinline__ void tile_each(const Ctx &C, F f) {
+  const KParams &P = *C.P;
+  const int cnt = own_tiles(P.ntiles);
+  for (int m = 0; m < cnt; ++m) {
+    const int i = own_tile(m, cnt, C.rev) * TILE + threadIdx.x;
     if (i < P.n) f(i);
   }
 }
@@ -119,10 +137,10 @@ __device__ __forceinline__ void tile_each(const KParams &P, F f) {
 template <int K, class F>
 __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
   const KParams &P = *C.P;
-  const int G = vnb(), nt = P.ntiles, B = vbid();
+  const int nt = P.ntiles, cnt = own_tiles(nt), rev = C.rev;
   if (!reduce) {
-    for (int t = B; t < nt; t += G) {
-      const int i = t * TILE + threadIdx.x;
+    for (int m = 0; m < cnt; ++m) {
+      const int i = own_tile(m, cnt, rev) * TILE + threadIdx.x;
       double v[K];
       if (i < P.n) f(i, v);
     }
@@ -131,10 +149,10 @@ __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double *part = C.part_w();
   C.pw ^= 1;
-  for (int t0 = B; t0 < nt; t0 += MAXTL * G) {   // chunks of at most MAXTL tiles
-    int tl = 0;
-    for (int t = t0; t < nt && tl < MAXTL; t += G, ++tl) {
-      const int i = t * TILE + threadIdx.x;
+  for (int m0 = 0; m0 < cnt; m0 += MAXTL) {   // chunks of at most MAXTL tiles
+    const int tn = min(MAXTL, cnt - m0);
+    for (int tl = 0; tl < tn; ++tl) {
+      const int i = own_tile(m0 + tl, cnt, rev) * TILE + threadIdx.x;
       double v[K];
 #pragma unroll
       for (int k = 0; k < K; ++k) v[k] = 0.0;
@@ -147,14 +165,14 @@ __device__ __forceinline__ void tile_phase(Ctx &C, bool reduce, F f) {
       }
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < tl * K; q += TPB) {
+    for (int q = threadIdx.x; q < tn * K; q += TPB) {
       const double *w = C.ws + q * 8;
       double a0 = w[0] + w[4], a1 = w[1] + w[5];
       const double a2 = w[2] + w[6], a3 = w[3] + w[7];
       a0 = a0 + a2;
       a1 = a1 + a3;
       a0 = a0 + a1;
-      const int k = q % K, t = t0 + (q / K) * G;
+      const int k = q % K, t = own_tile(m0 + q / K, cnt, rev);
       part[(size_t)k * nt + t] = a0;
     }
     __syncthreads();
@@ -170,27 +188,26 @@ struct CgRows {
   static constexpr int R = (sizeof(T) == 4) ? 2 : 1;
 };
 
-// tile_phase over R tiles at a time: CTA B takes its tiles B, B+G, B+2G, ...
-// R by R, thread t row t of each (ii[r], ok[r] false past the mesh, where
-// ii[r] is a valid row to read from); the per-tile reductions are those of
-// tile_phase (each tile's canonical tree).
+// tile_phase over R tiles at a time: the CTA takes its tiles (in the phase's
+// direction) R by R, thread t row t of each (ii[r], ok[r] false past the
+// mesh, where ii[r] is a valid row to read from); the per-tile reductions are
+// those of tile_phase (each tile's canonical tree).
 template <int K, int R, class F>
 __device__ __forceinline__ void tile_phase_rows(Ctx &C, bool reduce, F f) {
   const KParams &P = *C.P;
-  const int G = vnb(), nt = P.ntiles, B = vbid();
+  const int nt = P.ntiles, cnt = own_tiles(nt), rev = C.rev;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double *part = C.part_w();
   if (reduce) C.pw ^= 1;
-  for (int t0 = B; t0 < nt; t0 += MAXTL * G) {
-    int tl = 0;
-    for (int t = t0; t < nt && tl < MAXTL; t += R * G, tl += R) {
+  for (int m0 = 0; m0 < cnt; m0 += MAXTL) {
+    const int tn = min(MAXTL, cnt - m0);
+    for (int tl = 0; tl < tn; tl += R) {
       int ii[R];
       bool ok[R], tv[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int tr = t + r * G;
-        tv[r] = tr < nt && tl + r < MAXTL;
-        const int i = tr * TILE + threadIdx.x;
+        tv[r] = tl + r < tn;
+        const int i = (tv[r] ? own_tile(m0 + tl + r, cnt, rev) : 0) * TILE + threadIdx.x;
         ok[r] = tv[r] && i < P.n;
         ii[r] = ok[r] ? i : 0;
       }
@@ -214,16 +231,15 @@ __device__ __forceinline__ void tile_phase_rows(Ctx &C, bool reduce, F f) {
         }
     }
     if (!reduce) continue;
-    const int ntl = min(MAXTL, (nt - t0 + G - 1) / G);
     __syncthreads();
-    for (int q = threadIdx.x; q < ntl * K; q += TPB) {
+    for (int q = threadIdx.x; q < tn * K; q += TPB) {
       const double *w = C.ws + q * 8;
       double a0 = w[0] + w[4], a1 = w[1] + w[5];
       const double a2 = w[2] + w[6], a3 = w[3] + w[7];
       a0 = a0 + a2;
       a1 = a1 + a3;
       a0 = a0 + a1;
-      const int k = q % K, t = t0 + (q / K) * G;
+      const int k = q % K, t = own_tile(m0 + q / K, cnt, rev);
       part[(size_t)k * nt + t] = a0;
     }
     __syncthreads();
@@ -558,7 +574,7 @@ __device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<
     }
     auto gets = [&](int j, int d) -> T {
       const size_t k = (size_t)j * NS + d;
-      return (T)((double)r[k] + (-alpha[d]) * (double)vn[k]);
+      return vaxpy<T>(r[k], -alpha[d], vn[k]);
     };
     // D: s, x += alpha p, q = A s, M^{-1} row-local part
     C.phase(PH_KRY_SPMV);
@@ -570,7 +586,7 @@ __device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<
         si[d] = gets(i, d);
         if (active & (1u << d)) {
           w.s[k] = si[d];
-          w.x[k] = (T)((double)w.x[k] + alpha[d] * (double)pn[k]);
+          w.x[k] = vaxpy<T>(w.x[k], alpha[d], pn[k]);
         }
       }
       spmv_row<NS>(A, i, gets, y);
@@ -609,9 +625,8 @@ __device__ __forceinline__ bool bicgstab(Ctx &C, const MatT<T> &A, const KWorkT<
         const size_t k = (size_t)i * NS + d;
         double rv = (double)r[k];
         if (active & (1u << d)) {
-          const double sv = (double)w.s[k];
-          w.x[k] = (T)((double)w.x[k] + omega[d] * sv);
-          const T rt = (T)(sv + (-omega[d]) * (double)w.t[k]);
+          w.x[k] = vaxpy<T>(w.x[k], omega[d], w.s[k]);
+          const T rt = vaxpy<T>(w.s[k], -omega[d], w.t[k]);
           r[k] = rt;
           rv = (double)rt;
         }
@@ -692,7 +707,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
     auto getp = [&](int j, int d) -> T {
       const size_t k = (size_t)j * NS + d;
       if (first) return z[k];
-      return (T)((double)z[k] + beta[d] * (double)po[k]);
+      return vaxpy<T>(z[k], beta[d], po[k]);
     };
     // A: p update, q = A p, <p,q>
     C.phase(PH_KRY_SPMV);
@@ -743,7 +758,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
     T *ro = w.r[rc], *rn = w.r[rc ^ 1];
     auto getr = [&](int j, int d) -> T {
       const size_t k = (size_t)j * NS + d;
-      return (T)((double)ro[k] + (-alpha[d]) * (double)w.q[k]);
+      return vaxpy<T>(ro[k], -alpha[d], w.q[k]);
     };
     // B: x, r updates and M^{-1} levels 0/1
     C.phase(PH_KRY_PREC);
@@ -766,7 +781,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
               const size_t k = (size_t)i * NS + d;
               rr[r][d] = getr(i, d);
               if (ok[r] && (active & (1u << d))) {
-                w.x[k] = (T)((double)w.x[k] + alpha[d] * (double)pn[k]);
+                w.x[k] = vaxpy<T>(w.x[k], alpha[d], pn[k]);
                 rn[k] = rr[r][d];
               }
             }
@@ -813,7 +828,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
         const size_t k = (size_t)i * NS + d;
         rr[d] = getr(i, d);
         if (active & (1u << d)) {
-          w.x[k] = (T)((double)w.x[k] + alpha[d] * (double)pn[k]);
+          w.x[k] = vaxpy<T>(w.x[k], alpha[d], pn[k]);
           rn[k] = rr[d];
         }
       }
@@ -1009,7 +1024,7 @@ __device__ __forceinline__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> 
 #pragma unroll
         for (int d = 0; d < NS; ++d) {
           const size_t q = (size_t)i * NS + d;
-          const T qv = (T)((double)qn[q] + (-h[d]) * (double)Vp[q]);
+          const T qv = vaxpy<T>(qn[q], -h[d], Vp[q]);
           qn[q] = qv;
           v[d] = norm ? (double)qv * (double)qv : (double)Vm[q] * (double)qv;
         }
@@ -1085,7 +1100,7 @@ __device__ __forceinline__ bool gmres(Ctx &C, const MatT<T> &A, const KWorkT<T> 
       }
     }
     __syncthreads();
-    tile_each(P, [&](int i) {
+    tile_each(C, [&](int i) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         if (!(ran & (1u << d))) continue;
@@ -1346,7 +1361,7 @@ __device__ __forceinline__ bool gradient_p(Ctx &C, bool correct_u) {
   for (int pass = 0; pass < npass; ++pass) {
     const bool last = (pass == npass - 1);
     C.phase(PH_GRAD);
-    tile_each(P, [&](int i) {
+    tile_each(C, [&](int i) {
       double g[NS];
       green_gauss_row<NS>(P, P.pf, i, g);
       st<NS>(P.gp, i, g);
@@ -1541,7 +1556,7 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
   const double nu = P.nu;
   // production, destruction, effective diffusivities (turbulence!, :256-272)
   C.phase(PH_TURB);
-  tile_each(P, [&](int i) {
+  tile_each(C, [&](int i) {
     double g[3][3];
     grad_u_row<NS>(P, i, g);
 #pragma unroll
@@ -1596,7 +1611,7 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
     double *phi = om ? P.w : P.k;
     const KCfg &cfg = om ? P.kW : P.kK;
     C.phase(PH_TURB);
-    tile_each(P, [&](int i) {
+    tile_each(C, [&](int i) {
       double b[1];
       b[0] = om ? scalar_row(P, P.AP, i, phi, P.nueffw, P.Dw, P.Pw, P.bcW, P.aW, P.divW, P.timeW, true)
                 : scalar_row(P, P.AP, i, phi, P.nueffk, P.Dk, P.Pk, P.bcK, P.aK, P.divK, P.timeK, false);
@@ -1610,7 +1625,7 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
     if (!krylov<1, T>(C, A, wk, P.bP, cfg, cfg.solver, its, rn)) return false;
     // run! copy-back, then constrain_boundary! for omega (:401-448)
     C.phase(PH_TURB);
-    tile_each(P, [&](int i) {
+    tile_each(C, [&](int i) {
       double v = (double)wk.x[i] + phi[i];
       if (om) {
         const FieldBC &bc = P.bcW;
@@ -1624,7 +1639,7 @@ __device__ __forceinline__ bool turbulence(Ctx &C) {
     });
     if (!C.sync()) return false;
     for (int l = 0; l < P.nfl; ++l) {   // bound!(phi, eps()); after k also nut = k/omega
-      tile_each(P, [&](int i) {
+      tile_each(C, [&](int i) {
         if (ldro(P.flev + i) != l) return;
         bound_row(P, phi, i);
         if (!om) P.nut[i] = P.k[i] / P.w[i];
@@ -1679,7 +1694,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
     const MatT<T> &AUT = matU<T>(P);
     const KWorkT<T> &wU = workU<T>(P);
     C.phase(PH_MOM_ASM);
-    tile_each(P, [&](int i) {
+    tile_each(C, [&](int i) {
       double b[NS];
       momentum_row<NS>(P, i, !piso, b);
       krylov_init_row<NS, T>(P, P.AU, AUT, wU, b, P.U, i, P.kU.solver);
@@ -1693,7 +1708,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
     for (int d = 0; d < NS; ++d) finite = finite && isfinite(rnU[d]);
     // run! copy-back: U = x + x0
     C.phase(PH_UPDATE);
-    tile_each(P, [&](int i) {
+    tile_each(C, [&](int i) {
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         const size_t k = (size_t)i * NS + d;
@@ -1736,7 +1751,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
     for (int corr = 0; corr < ncorr; ++corr) {
       if (corr > 0) {   // H! again with the corrected U (PISO corrector loop)
         C.phase(PH_RESID);
-        tile_each(P, [&](int i) {
+        tile_each(C, [&](int i) {
           double bb[NS];
           ld<NS>(P.bU, i, bb);
           H_row<NS>(P, i, bb);
@@ -1759,7 +1774,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
       const MatT<T> &APT = matP<T>(P);
       const KWorkT<T> &wP = workP<T>(P);
       C.phase(PH_P_ASM);
-      tile_each(P, [&](int i) {
+      tile_each(C, [&](int i) {
         double b[1];
         b[0] = pressure_row<NS>(P, i);
         krylov_init_row<1, T>(P, P.AP, APT, wP, b, P.p, i, P.kP.solver);
@@ -1772,7 +1787,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
       finite = finite && isfinite(rnP[0]);
       // run! copy-back then explicit_relaxation!(p, prev, alpha_p)
       C.phase(PH_UPDATE);
-      tile_each(P, [&](int i) {
+      tile_each(C, [&](int i) {
         const double pn = (double)wP.x[i] + P.p[i];
         const double p0 = P.p[i];
         P.p[i] = p0 + P.aP * (pn - p0);
@@ -1833,7 +1848,7 @@ __device__ __forceinline__ void simple_program(Ctx &C, int iters, bool piso) {
 __device__ __forceinline__ void solve_program(Ctx &C) {
   const KParams &P = *C.P;
   C.phase(PH_P_ASM);
-  tile_each(P, [&](int i) {
+  tile_each(C, [&](int i) {
     double b[1] = {P.sb[i]};
     krylov_init_row<1, double>(P, P.AU, P.AU, P.wU, b, P.U, i, P.solve_solver);
   });
@@ -1847,7 +1862,7 @@ __device__ __forceinline__ void solve_program(Ctx &C) {
   int its[1];
   double rn[1];
   if (!krylov<1, double>(C, P.AU, P.wU, P.sb, cfg, P.solve_solver, its, rn)) return;
-  tile_each(P, [&](int i) { P.U[i] = P.wU.x[i] + P.U[i]; });
+  tile_each(C, [&](int i) { P.U[i] = P.wU.x[i] + P.U[i]; });
   if (vbid() == 0 && threadIdx.x == 0) {
     P.solve_out[0] = (double)its[0];
     P.solve_out[1] = rn[0];
@@ -1887,6 +1902,7 @@ __global__ void __launch_bounds__(TPB, MB) xcal_program_kernel(const __grid_cons
   C.S.ok = &sm_ok;
   C.part = prm.part;
   C.pw = 0;
+  C.rev = 0;
   C.sm = sm;
   C.sm_out = sm_out;
   C.ws = ws;
@@ -2017,6 +2033,7 @@ __global__ void __launch_bounds__(TPB, MB) xcal_serve_kernel(ServeMail *mail, co
     C.S.ok = &sm_ok;
     C.part = sP.part;
     C.pw = 0;
+    C.rev = 0;
     C.sm = sm;
     C.sm_out = sm_out;
     C.ws = ws;

@@ -129,7 +129,7 @@ struct Job {
 struct xcal_server_s {
   int device = 0;
   xcal_serve_cfg cfg{};
-  int tiles_per_cta = 2, max_ctas = 64;
+  int tiles_per_cta = 4, max_ctas = 64;
   // device arena, pinned host arena (with its device view), barrier words
   char *dev_arena = nullptr;
   char *host_arena = nullptr, *host_arena_dev = nullptr;
