@@ -188,6 +188,10 @@ template <typename T>
 struct CgRows {
   static constexpr int R = 2;
 };
+// Row pairs pay when the CTAs hold two tiles or more each; with one tile per
+// CTA or fewer (small meshes: one phase is a barrier and one row per thread)
+// the one-row routines are faster.  Uniform across the CTAs of a run.
+__device__ __forceinline__ bool pairs_pay(const KParams &P) { return P.ntiles >= 2 * vnb(); }
 
 // tile_phase over R tiles at a time: the CTA takes its tiles (in the phase's
 // direction) R by R, thread t row t of each (ii[r], ok[r] false past the
@@ -315,7 +319,7 @@ __device__ __forceinline__ bool precon_tail(Ctx &C, const MatT<T> &A, const T *i
   const int nph = precon_tail_phases(P, A, setup, first_lvl);
   C.phase(setup ? PH_PREC_SETUP : PH_KRY_PREC);
   if constexpr (R > 1) {
-    if (!setup && A.precon == PRECON_DILU && nph > 0) {
+    if (!setup && A.precon == PRECON_DILU && nph > 0 && pairs_pay(P)) {
       // the DILU levels R rows at a time; in a warp holding a row of the
       // level, rows outside it compute with what they read and store
       // nothing; a warp without one skips the rows (with a level-ordered
@@ -712,7 +716,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
     };
     // A: p update, q = A p, <p,q>
     C.phase(PH_KRY_SPMV);
-    if constexpr (CgRows<T>::R > 1) {
+    if (CgRows<T>::R > 1 && pairs_pay(P)) {
       constexpr int R = CgRows<T>::R;
       tile_phase_rows<NS, R>(C, true, [&](const int (&ii)[R], const bool (&ok)[R], double (&v)[R][NS]) {
         T y[R][NS];
@@ -763,7 +767,7 @@ __device__ __forceinline__ bool cg(Ctx &C, const MatT<T> &A, const KWorkT<T> &w,
     };
     // B: x, r updates and M^{-1} levels 0/1
     C.phase(PH_KRY_PREC);
-    if constexpr (CgRows<T>::R > 1) {
+    if (CgRows<T>::R > 1 && pairs_pay(P)) {
       if (A.precon == PRECON_DILU && !fuse) {
         // R rows at a time; a DILU row of level 0 or 1 is one forward row
         // (level 0: no lower neighbours, then its diagonal step when it has
